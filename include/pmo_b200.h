@@ -1,0 +1,240 @@
+/*
+ * pmo_b200.h — C ABI of the B200 voxel Monte Carlo photon-transport engine.
+ *
+ * Everything here is plain C: device pointers, sizes and a cudaStream_t passed
+ * as an opaque pointer.  Every entry point is stream-ordered and asynchronous:
+ * it validates its arguments on the host, enqueues work on `stream` and
+ * returns a status code without synchronising.  Device-side faults that can
+ * only be seen while photons run (a photon that exceeds its event cap, a step
+ * out of the volume, a label without optical properties) are counted in the
+ * caller's `counters` buffer; `pmo_check_counters` turns those counts into a
+ * status code after the caller has synchronised the stream.
+ *
+ * Photon p of a run draws all its random numbers from Philox4x32-10
+ * (Salmon et al., SC'11) with key = (seed_lo, seed_hi) and counter
+ * (n, stream, p_lo, p_hi): stream 0 gives the four uniforms of interaction n
+ * (step length, roulette, Henyey-Greenstein cos(theta), azimuth), stream 1
+ * word 0 the uniform of the n-th Fresnel decision, stream 2 the source
+ * uniforms.  A photon's history therefore depends only on (seed, p, optics),
+ * never on the launch shape, so runs over photon ranges can be split, resumed
+ * and replayed.
+ *
+ * Label volume layout follows the reference: C-order (nx, ny, nz) uint8
+ * array, linear index (ix*ny + iy)*nz + iz, padded by a one-voxel shell of
+ * `end_label` on all six faces (pymopt/voxel_gpu/_classes.py:439-459).
+ */
+#ifndef PMO_B200_H
+#define PMO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PMO_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+#define PMO_OK                 0
+#define PMO_ERR_ARG            1   /* bad argument (null pointer, size, range) */
+#define PMO_ERR_GEOMETRY       2   /* a photon stepped outside the volume       */
+#define PMO_ERR_LABEL          3   /* a photon entered a label without optics   */
+#define PMO_ERR_STEP_CAP       4   /* a photon exceeded max_events              */
+#define PMO_ERR_CUDA           5   /* a CUDA runtime call failed                */
+#define PMO_ERR_WORKSPACE      6   /* workspace missing or too small            */
+#define PMO_ERR_TIMEOUT        7   /* a bounded device wait gave up             */
+#define PMO_ERR_NUMERIC        8   /* a non-finite weight or direction appeared */
+
+/* ---- precision of the transport arithmetic ----------------------------- */
+#define PMO_FP32 0               /* the product path                           */
+#define PMO_FP64 1               /* the per-photon FP64 build (validation)     */
+
+/* ---- photon sources ----------------------------------------------------- */
+#define PMO_SRC_PENCIL   0       /* every photon starts at (ix,iy,iz, p, v, w0) */
+#define PMO_SRC_GAUSSIAN 1       /* pencil + lateral N(0, sigma^2) in x and y    */
+#define PMO_SRC_STATE    2       /* per-photon initial state arrays (cuVMC form) */
+
+/* ---- optical-property modes --------------------------------------------- */
+#define PMO_PROPS_LABEL  0       /* ma/ms/g/n indexed by voxel label            */
+#define PMO_PROPS_VOXEL  1       /* ma/ms per voxel, g/n per label              */
+
+/* ---- fluence tally modes ------------------------------------------------ */
+#define PMO_FLU_NONE     0
+#define PMO_FLU_GLOBAL   1       /* fp32 atomics straight to the padded grid    */
+#define PMO_FLU_SHARED   2       /* + per-block shared-memory window            */
+
+/* ---- ledger slots (double), accumulated by the kernels ------------------ */
+#define PMO_L_WINIT      0       /* sum of launched photon weights              */
+#define PMO_L_RD         1       /* exit weight with v_z < 0 (reference Rd)     */
+#define PMO_L_TT         2       /* exit weight with v_z > 0 (reference Tt)     */
+#define PMO_L_EXIT0      3       /* exit weight with v_z == 0                    */
+#define PMO_L_ABS        4       /* absorbed weight                              */
+#define PMO_L_RGAIN      5       /* weight created by roulette survival          */
+#define PMO_L_RLOSS      6       /* weight removed by roulette death             */
+#define PMO_L_ERRW       7       /* weight of photons killed by an error         */
+#define PMO_L_RD_TOP     8       /* exit weight through a -z face                */
+#define PMO_L_TT_BOTTOM  9       /* exit weight through a +z face                */
+#define PMO_L_SPEC       10      /* specular weight of source-reflected photons  */
+#define PMO_LEDGER_N     16
+
+/* ---- event counters (unsigned long long) -------------------------------- */
+#define PMO_C_PHOTONS    0       /* photons finished                             */
+#define PMO_C_INTERACT   1       /* interactions (hop-drop-spin cycles)          */
+#define PMO_C_CROSS      2       /* voxel-face crossings                         */
+#define PMO_C_FRESNEL    3       /* Fresnel evaluations (index mismatch)         */
+#define PMO_C_REFLECT    4       /* Fresnel/TIR reflections                      */
+#define PMO_C_ROULETTE   5       /* roulette draws                               */
+#define PMO_C_EXITS      6       /* photons that left through the end label      */
+#define PMO_C_ERR_GEOM   7
+#define PMO_C_ERR_LABEL  8
+#define PMO_C_ERR_CAP    9
+#define PMO_C_ERR_NUM    10
+#define PMO_C_SAMECROSS  11      /* crossings into a voxel of the same label     */
+#define PMO_COUNTERS_N   16
+
+/* ---- R(r) / T(r) histogram categories, layout [PMO_RR_CATS][nr] --------- */
+#define PMO_RR_TOP       0       /* exits through a -z face                      */
+#define PMO_RR_BOTTOM    1       /* exits through a +z face                      */
+#define PMO_RR_LAT_NEG   2       /* exits through an x/y face with v_z < 0       */
+#define PMO_RR_LAT_POS   3       /* exits through an x/y face with v_z > 0       */
+#define PMO_RR_CATS      4
+
+/* ---- run flags ---------------------------------------------------------- */
+#define PMO_FLAG_EXPORT_EXITS  1u  /* write per-photon final state arrays        */
+#define PMO_FLAG_PHOTON_STATS  2u  /* write per-photon event counts (validation) */
+
+typedef struct pmo_problem {
+    /* geometry: padded label volume, C-order (nx, ny, nz) */
+    const uint8_t *labels;
+    int32_t nx, ny, nz;
+    float voxel_space;           /* l [mm] */
+    int32_t end_label;           /* shell label; photons leave when they enter it */
+
+    /* optics: per-label tables of n_labels entries (n_labels <= 256);
+       n[end_label] is the ambient refractive index. */
+    int32_t props_mode;          /* PMO_PROPS_LABEL or PMO_PROPS_VOXEL */
+    int32_t n_labels;
+    const float *ma, *ms, *g, *n;
+    const float *vox_ma, *vox_ms; /* PMO_PROPS_VOXEL: nx*ny*nz each */
+
+    /* source */
+    int32_t source;              /* PMO_SRC_* */
+    int32_t src_ix, src_iy, src_iz;
+    float src_p[3], src_v[3];
+    float src_w0;                /* initial weight of transported photons */
+    float beam_sigma;            /* PMO_SRC_GAUSSIAN: sigma of x and y [mm] */
+    float spec_prob;             /* probability that the source photon is reflected
+                                    specularly before entering (w = 1, v = spec_v) */
+    float spec_v[3];
+    int32_t center_ix, center_iy; /* exit-position origin (reference _encooder) */
+    /* PMO_SRC_STATE: SoA arrays of 3*count (add, p, v) and count (w),
+       indexed by photon - photon_begin; final states are written back. */
+    int32_t *state_add;
+    float *state_p, *state_v, *state_w;
+
+    /* photons */
+    uint64_t seed;
+    uint64_t photon_begin, photon_count;
+    uint32_t max_events;         /* per-photon event cap, 0 = default (2^26) */
+    int32_t precision;           /* PMO_FP32 or PMO_FP64 */
+    uint32_t flags;              /* PMO_FLAG_* */
+} pmo_problem;
+
+typedef struct pmo_tallies {
+    double *ledger;                   /* PMO_LEDGER_N doubles, accumulated */
+    unsigned long long *counters;     /* PMO_COUNTERS_N, accumulated */
+    float *rr;                        /* PMO_RR_CATS * nr, accumulated, or NULL */
+    int32_t nr;
+    float dr;                         /* bin width [mm]; bins (i*dr, (i+1)*dr] */
+    int32_t fluence_mode;             /* PMO_FLU_* */
+    float *absorbed;                  /* nx*ny*nz absorbed weight, accumulated */
+    int32_t win_lo[3];                /* PMO_FLU_SHARED: window origin (voxel) */
+    int32_t win_dim[3];               /* PMO_FLU_SHARED: window extent (voxels) */
+    /* PMO_FLAG_EXPORT_EXITS: final state per photon (index photon - begin).
+       add/p/v are SoA 3*photon_count; killed photons are all zero as in the
+       reference (pymopt/voxel_gpu/_cukernel.py:182-190). */
+    int32_t *exit_add;
+    float *exit_p, *exit_v, *exit_w;
+    /* PMO_FLAG_PHOTON_STATS: per-photon interaction / crossing / Fresnel counts */
+    uint32_t *ph_interact, *ph_cross, *ph_fresnel;
+} pmo_tallies;
+
+typedef struct pmo_launch {
+    int32_t block_threads;       /* 0 = default */
+    int32_t blocks_per_sm;       /* 0 = occupancy maximum */
+} pmo_launch;
+
+/* Library identity. */
+int pmo_abi_version(void);
+const char *pmo_status_string(int status);
+int pmo_device_info(int *sm_count, int *cc_major, int *cc_minor);
+
+/* Bytes of device scratch the caller passes as `workspace` to the run
+   entry points (work counters; contents need not be initialised; the entry
+   points clear what they use, stream-ordered).  pmo_cuvmc, whose reference
+   signature has no tally arguments, leaves its ledger (PMO_LEDGER_N doubles)
+   and counters (PMO_COUNTERS_N unsigned long long) in the workspace at the
+   byte offsets below. */
+#define PMO_WS_LEDGER_OFFSET   64
+#define PMO_WS_COUNTERS_OFFSET 256
+size_t pmo_workspace_bytes(void);
+
+/*
+ * Forward transport with on-device tallies.
+ * Replaces the launch of cuVMC in BaseVoxelMonteCarlo.start
+ * (pymopt/voxel_gpu/_classes.py:105-111) together with the host reductions
+ * that follow it: getRdTtRate (pymopt/voxel_gpu/_classes.py:326-334) and
+ * metrics.radialDistance (pymopt/metrics/_scoring.py:16-25).
+ * Tallies are accumulated, never cleared, so consecutive runs over photon
+ * ranges [a, b), [b, c) with one seed equal one run over [a, c).
+ */
+int pmo_run_plain(const pmo_problem *prob, const pmo_tallies *tal,
+                  const pmo_launch *launch, void *workspace,
+                  size_t workspace_bytes, void *stream);
+
+/*
+ * Drop-in for the reference kernel cuVMC (pymopt/voxel_gpu/_cukernel.py:27-35):
+ * same argument list and meaning (SoA state add[3*nPh], p[3*nPh], v[3*nPh],
+ * w[nPh] updated in place; ma/ms/g indexed by label < end_point; n indexed
+ * by label <= end_point; voxel index (x*M + y)*L + z), plus `nx`
+ * (voxel_model.shape[0], for bounds checking), a workspace and a stream.
+ * The random stream is the Philox scheme above with seed = rand_seed.
+ */
+int pmo_cuvmc(int32_t *add, float *p, float *v, float *w,
+              const float *ma, const float *ms, const float *n, const float *g,
+              const int8_t *voxel_model, float l, int32_t M, int32_t L,
+              int32_t nPh, int8_t end_point, int32_t rand_seed, int32_t nx,
+              void *workspace, size_t workspace_bytes, void *stream);
+
+/*
+ * Fluence normalisation in FP64: phi = absorbed / (n_photons * l^3 * mu_a)
+ * over the interior (nx-2, ny-2, nz-2) of the padded grid; voxels with
+ * mu_a == 0 get 0.  mu_a comes from the label table or the voxel grid of
+ * `prob`.  No counterpart in the reference GPU path (the reference tallies
+ * fluence only in pymopt/fluence/intarnal_fluence.py:12-152, on the host).
+ */
+int pmo_normalize_fluence(const pmo_problem *prob, const float *absorbed,
+                          double n_photons, double *phi_out, void *stream);
+
+/* Philox4x32-10 words of the engine's generator for n counters ctr[4*n]
+   (device arrays) under key (key0, key1): known-answer checks of the random
+   stream layout.  No counterpart in the reference (it uses cuRAND XORWOW,
+   pymopt/voxel_gpu/_cukernel.py:42-43). */
+int pmo_philox_words(const uint32_t *ctr, uint32_t key0, uint32_t key1,
+                     uint32_t *out, int n, void *stream);
+
+/* cuRAND's Philox4_32_10 for comparison: words of curand4() after
+   curand_init(seed, subsequence[i], 4 * block[i]). */
+int pmo_philox_words_curand(unsigned long long seed,
+                            const unsigned long long *subsequence,
+                            const unsigned long long *block, uint32_t *out,
+                            int n, void *stream);
+
+/* Turn device-side counters (after the caller synchronised) into a status. */
+int pmo_check_counters(const unsigned long long *host_counters);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PMO_B200_H */

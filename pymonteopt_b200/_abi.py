@@ -1,0 +1,139 @@
+"""ctypes mirror of ``include/pmo_b200.h``.
+
+The constants and struct layouts here must match the C header; a CPU test
+parses the header and compares every ``#define`` and field.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+PMO_ABI_VERSION = 1
+
+# status codes
+PMO_OK = 0
+PMO_ERR_ARG = 1
+PMO_ERR_GEOMETRY = 2
+PMO_ERR_LABEL = 3
+PMO_ERR_STEP_CAP = 4
+PMO_ERR_CUDA = 5
+PMO_ERR_WORKSPACE = 6
+PMO_ERR_TIMEOUT = 7
+PMO_ERR_NUMERIC = 8
+
+PMO_FP32 = 0
+PMO_FP64 = 1
+
+PMO_SRC_PENCIL = 0
+PMO_SRC_GAUSSIAN = 1
+PMO_SRC_STATE = 2
+
+PMO_PROPS_LABEL = 0
+PMO_PROPS_VOXEL = 1
+
+PMO_FLU_NONE = 0
+PMO_FLU_GLOBAL = 1
+PMO_FLU_SHARED = 2
+
+PMO_L_WINIT = 0
+PMO_L_RD = 1
+PMO_L_TT = 2
+PMO_L_EXIT0 = 3
+PMO_L_ABS = 4
+PMO_L_RGAIN = 5
+PMO_L_RLOSS = 6
+PMO_L_ERRW = 7
+PMO_L_RD_TOP = 8
+PMO_L_TT_BOTTOM = 9
+PMO_L_SPEC = 10
+PMO_LEDGER_N = 16
+
+PMO_C_PHOTONS = 0
+PMO_C_INTERACT = 1
+PMO_C_CROSS = 2
+PMO_C_FRESNEL = 3
+PMO_C_REFLECT = 4
+PMO_C_ROULETTE = 5
+PMO_C_EXITS = 6
+PMO_C_ERR_GEOM = 7
+PMO_C_ERR_LABEL = 8
+PMO_C_ERR_CAP = 9
+PMO_C_ERR_NUM = 10
+PMO_C_SAMECROSS = 11
+PMO_COUNTERS_N = 16
+
+PMO_RR_TOP = 0
+PMO_RR_BOTTOM = 1
+PMO_RR_LAT_NEG = 2
+PMO_RR_LAT_POS = 3
+PMO_RR_CATS = 4
+
+PMO_FLAG_EXPORT_EXITS = 1
+PMO_FLAG_PHOTON_STATS = 2
+
+PMO_WS_LEDGER_OFFSET = 64
+PMO_WS_COUNTERS_OFFSET = 256
+
+STATUS_NAMES = {
+    PMO_OK: "ok",
+    PMO_ERR_ARG: "bad argument",
+    PMO_ERR_GEOMETRY: "photon stepped outside the volume",
+    PMO_ERR_LABEL: "photon entered a label without optical properties",
+    PMO_ERR_STEP_CAP: "photon exceeded its event cap",
+    PMO_ERR_CUDA: "CUDA runtime error",
+    PMO_ERR_WORKSPACE: "workspace missing or too small",
+    PMO_ERR_TIMEOUT: "bounded device wait timed out",
+    PMO_ERR_NUMERIC: "non-finite weight or direction",
+}
+
+_fp = C.POINTER(C.c_float)
+_ip = C.POINTER(C.c_int32)
+_up = C.POINTER(C.c_uint32)
+
+
+class PmoProblem(C.Structure):
+    _fields_ = [
+        ("labels", C.c_void_p),
+        ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+        ("voxel_space", C.c_float),
+        ("end_label", C.c_int32),
+        ("props_mode", C.c_int32),
+        ("n_labels", C.c_int32),
+        ("ma", C.c_void_p), ("ms", C.c_void_p), ("g", C.c_void_p), ("n", C.c_void_p),
+        ("vox_ma", C.c_void_p), ("vox_ms", C.c_void_p),
+        ("source", C.c_int32),
+        ("src_ix", C.c_int32), ("src_iy", C.c_int32), ("src_iz", C.c_int32),
+        ("src_p", C.c_float * 3), ("src_v", C.c_float * 3),
+        ("src_w0", C.c_float),
+        ("beam_sigma", C.c_float),
+        ("spec_prob", C.c_float),
+        ("spec_v", C.c_float * 3),
+        ("center_ix", C.c_int32), ("center_iy", C.c_int32),
+        ("state_add", C.c_void_p), ("state_p", C.c_void_p),
+        ("state_v", C.c_void_p), ("state_w", C.c_void_p),
+        ("seed", C.c_uint64),
+        ("photon_begin", C.c_uint64), ("photon_count", C.c_uint64),
+        ("max_events", C.c_uint32),
+        ("precision", C.c_int32),
+        ("flags", C.c_uint32),
+    ]
+
+
+class PmoTallies(C.Structure):
+    _fields_ = [
+        ("ledger", C.c_void_p),
+        ("counters", C.c_void_p),
+        ("rr", C.c_void_p),
+        ("nr", C.c_int32),
+        ("dr", C.c_float),
+        ("fluence_mode", C.c_int32),
+        ("absorbed", C.c_void_p),
+        ("win_lo", C.c_int32 * 3),
+        ("win_dim", C.c_int32 * 3),
+        ("exit_add", C.c_void_p), ("exit_p", C.c_void_p),
+        ("exit_v", C.c_void_p), ("exit_w", C.c_void_p),
+        ("ph_interact", C.c_void_p), ("ph_cross", C.c_void_p), ("ph_fresnel", C.c_void_p),
+    ]
+
+
+class PmoLaunch(C.Structure):
+    _fields_ = [("block_threads", C.c_int32), ("blocks_per_sm", C.c_int32)]

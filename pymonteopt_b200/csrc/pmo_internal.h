@@ -1,0 +1,70 @@
+// pmo_internal.h — shared between the kernel translation units and the C ABI.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/pmo_b200.h"
+
+namespace pmo {
+
+// Everything a transport kernel reads, passed by value (kernel parameter
+// space).  Built by the C ABI from pmo_problem / pmo_tallies.
+struct KParams {
+    // geometry
+    const uint8_t *labels;
+    int32_t nx, ny, nz;
+    uint32_t sx, sy;               // strides of x and y in the label volume
+    float l;
+    int32_t end_label;
+    int32_t n_labels;
+    // optics
+    const float *ma, *ms, *g, *n;
+    const float *vox_ma, *vox_ms;
+    // source
+    int32_t source;
+    int32_t src_ix, src_iy, src_iz;
+    float src_p[3], src_v[3];
+    float src_w0, beam_sigma, spec_prob;
+    float spec_v[3];
+    int32_t cx, cy;
+    int32_t *state_add;
+    float *state_p, *state_v, *state_w;
+    // photons
+    uint32_t key0, key1;
+    uint64_t begin, count;
+    uint32_t max_events;
+    uint32_t flags;
+    // tallies
+    double *ledger;
+    unsigned long long *counters;
+    float *rr;
+    int32_t nr;
+    float dr;
+    int32_t rr_shared;             // histogram privatised in shared memory
+    float *absorbed;
+    int32_t win_lo[3], win_dim[3]; // shared fluence window (PMO_FLU_SHARED)
+    int32_t *exit_add;
+    float *exit_p, *exit_v, *exit_w;
+    uint32_t *ph_interact, *ph_cross, *ph_fresnel;
+    // scratch: [0] next photon chunk
+    unsigned long long *work;
+};
+
+// Launch configuration chosen by the caller or by the occupancy query.
+struct LaunchShape {
+    int block_threads;
+    int blocks;
+    size_t smem;
+};
+
+// vmc_plain.cu
+cudaError_t launch_plain(const KParams &kp, int precision, int props_mode, int fluence_mode,
+                         int block_threads, int blocks_per_sm, cudaStream_t stream,
+                         LaunchShape *shape_out);
+cudaError_t launch_normalize_fluence(const KParams &kp, int props_mode, const float *absorbed,
+                                     double n_photons, double *phi, cudaStream_t stream);
+
+size_t plain_smem_bytes(int precision, int nr, int rr_shared, int fluence_mode,
+                        const int32_t win_dim[3]);
+
+}  // namespace pmo

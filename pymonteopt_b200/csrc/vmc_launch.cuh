@@ -1,0 +1,65 @@
+// vmc_launch.cuh — persistent-grid launch of the transport kernel for one
+// arithmetic type.  Included by vmc_plain_f32.cu and vmc_plain_f64.cu, which
+// are compiled with different floating-point flags.
+#pragma once
+#include "vmc_transport.cuh"
+
+namespace pmo {
+
+inline int device_sm_count() {
+    static int cached[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    if (dev < 0 || dev >= 64) return 0;
+    if (!cached[dev]) {
+        int sms = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+            return 0;
+        cached[dev] = sms;
+    }
+    return cached[dev];
+}
+
+template <typename R, int PROPS, int FLU>
+cudaError_t launch_plain_t(const KParams &kp, int threads, int blocks_per_sm, cudaStream_t s,
+                           LaunchShape *out) {
+    auto kern = vmc_plain_kernel<R, PROPS, FLU>;
+    const size_t smem = SmemLayout<R>::total(kp.nr, kp.rr_shared, FLU, kp.win_dim);
+    cudaError_t e;
+    if (smem > 48 * 1024) {
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    const int sms = device_sm_count();
+    if (sms <= 0) return cudaErrorNoDevice;
+    int occ = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, smem);
+    if (e != cudaSuccess) return e;
+    if (occ < 1) return cudaErrorInvalidConfiguration;
+    const int per_sm = blocks_per_sm > 0 && blocks_per_sm < occ ? blocks_per_sm : occ;
+    uint64_t blocks = (uint64_t)sms * per_sm;
+    const uint64_t useful = (kp.count + threads - 1) / threads;
+    if (blocks > useful) blocks = useful > 0 ? useful : 1;
+    kern<<<(unsigned)blocks, threads, smem, s>>>(kp);
+    if (out) {
+        out->block_threads = threads;
+        out->blocks = (int)blocks;
+        out->smem = smem;
+    }
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_plain_r(const KParams &kp, int props, int flu, int threads, int bps,
+                           cudaStream_t s, LaunchShape *out) {
+    if (props == PMO_PROPS_LABEL) {
+        if (flu == PMO_FLU_NONE) return launch_plain_t<R, PMO_PROPS_LABEL, PMO_FLU_NONE>(kp, threads, bps, s, out);
+        if (flu == PMO_FLU_GLOBAL) return launch_plain_t<R, PMO_PROPS_LABEL, PMO_FLU_GLOBAL>(kp, threads, bps, s, out);
+        return launch_plain_t<R, PMO_PROPS_LABEL, PMO_FLU_SHARED>(kp, threads, bps, s, out);
+    }
+    if (flu == PMO_FLU_NONE) return launch_plain_t<R, PMO_PROPS_VOXEL, PMO_FLU_NONE>(kp, threads, bps, s, out);
+    if (flu == PMO_FLU_GLOBAL) return launch_plain_t<R, PMO_PROPS_VOXEL, PMO_FLU_GLOBAL>(kp, threads, bps, s, out);
+    return launch_plain_t<R, PMO_PROPS_VOXEL, PMO_FLU_SHARED>(kp, threads, bps, s, out);
+}
+
+}  // namespace pmo

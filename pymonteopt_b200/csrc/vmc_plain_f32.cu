@@ -1,0 +1,11 @@
+// vmc_plain_f32.cu — FP32 instantiation of the transport kernel (the product).
+// Compiled with -ftz=true -prec-div=false -prec-sqrt=false: single-precision
+// divides and square roots use the hardware approximations.
+#include "vmc_launch.cuh"
+
+namespace pmo {
+cudaError_t launch_plain_f32(const KParams &kp, int props, int flu, int threads, int bps,
+                             cudaStream_t s, LaunchShape *out) {
+    return launch_plain_r<float>(kp, props, flu, threads, bps, s, out);
+}
+}  // namespace pmo

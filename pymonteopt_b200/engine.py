@@ -1,0 +1,241 @@
+"""GPU engine: upload a :class:`~pymonteopt_b200.problem.TransportProblem`,
+run photon ranges through the C ABI, read tallies back.
+
+PyTorch supplies device memory and the current CUDA stream; all compute is in
+``libpmo_b200.so``.  Every call is stream-ordered on the current stream and
+asynchronous until a tally is read on the host.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+import torch
+
+from . import _abi as A
+from ._lib import PmoError, check, load
+
+
+def _ptr(t: Optional[torch.Tensor]):
+    return None if t is None else t.data_ptr()
+
+
+def _stream_handle(stream: Optional[torch.cuda.Stream] = None):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def require_cuda(device=None) -> torch.device:
+    if not torch.cuda.is_available():
+        raise RuntimeError("pymonteopt_b200 needs a CUDA device (B200, sm_100a); "
+                           "there is no CPU fallback")
+    d = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    if d.type != "cuda":
+        raise RuntimeError(f"device {d} is not a CUDA device")
+    return d
+
+
+class DeviceProblem:
+    """A problem whose volume and optical tables are resident on one GPU."""
+
+    def __init__(self, prob, device=None):
+        load()
+        self.device = require_cuda(device)
+        prob.validate()
+        self.host = prob
+        dev = self.device
+        self.labels = torch.from_numpy(prob.labels).to(dev)
+        self.ma = torch.from_numpy(prob.ma).to(dev)
+        self.ms = torch.from_numpy(prob.ms).to(dev)
+        self.g = torch.from_numpy(prob.g).to(dev)
+        self.n = torch.from_numpy(prob.n).to(dev)
+        self.vox_ma = self.vox_ms = None
+        if prob.vox_ma is not None:
+            self.vox_ma = torch.from_numpy(prob.vox_ma).to(dev)
+            self.vox_ms = torch.from_numpy(prob.vox_ms).to(dev)
+        self.workspace = torch.empty(int(load().pmo_workspace_bytes()), dtype=torch.uint8,
+                                     device=dev)
+
+    def set_optics(self, ma=None, ms=None, vox_ma=None, vox_ms=None) -> None:
+        """Replace optical properties in place (same shapes)."""
+        for name, val in (("ma", ma), ("ms", ms), ("vox_ma", vox_ma), ("vox_ms", vox_ms)):
+            if val is None:
+                continue
+            dst = getattr(self, name)
+            src = torch.as_tensor(val, dtype=torch.float32).reshape(dst.shape)
+            dst.copy_(src.to(self.device))
+
+    def struct(self, seed: int, begin: int, count: int, precision: int, flags: int = 0,
+               max_events: int = 0, state=None) -> A.PmoProblem:
+        s = A.PmoProblem()
+        self.host.fill_struct(s)
+        s.labels = self.labels.data_ptr()
+        s.ma, s.ms, s.g, s.n = (t.data_ptr() for t in (self.ma, self.ms, self.g, self.n))
+        if self.vox_ma is not None:
+            s.vox_ma, s.vox_ms = self.vox_ma.data_ptr(), self.vox_ms.data_ptr()
+        if state is not None:
+            s.source = A.PMO_SRC_STATE
+            s.state_add, s.state_p, s.state_v, s.state_w = (t.data_ptr() for t in state)
+        s.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
+        s.photon_begin = int(begin)
+        s.photon_count = int(count)
+        s.max_events = int(max_events)
+        s.precision = int(precision)
+        s.flags = int(flags)
+        return s
+
+
+@dataclass
+class TallySpec:
+    nr: int = 0
+    dr: float = 0.1
+    fluence: int = A.PMO_FLU_NONE
+    window: Optional[tuple] = None      # ((lo_x, lo_y, lo_z), (dim_x, dim_y, dim_z))
+    export_exits: bool = False
+    photon_stats: bool = False
+
+
+class Tallies:
+    """Device tally buffers of one run (accumulated across photon ranges)."""
+
+    def __init__(self, dprob: DeviceProblem, spec: TallySpec, n_photons: int):
+        dev = dprob.device
+        self.spec = spec
+        self.n_photons = 0
+        self.capacity = int(n_photons)
+        self.ledger = torch.zeros(A.PMO_LEDGER_N, dtype=torch.float64, device=dev)
+        self.counters = torch.zeros(A.PMO_COUNTERS_N, dtype=torch.int64, device=dev)
+        self.rr = (torch.zeros(A.PMO_RR_CATS, spec.nr, dtype=torch.float32, device=dev)
+                   if spec.nr > 0 else None)
+        self.absorbed = (torch.zeros(dprob.labels.shape, dtype=torch.float32, device=dev)
+                         if spec.fluence != A.PMO_FLU_NONE else None)
+        N = self.capacity
+        if spec.export_exits:
+            self.exit_add = torch.zeros(3, N, dtype=torch.int32, device=dev)
+            self.exit_p = torch.zeros(3, N, dtype=torch.float32, device=dev)
+            self.exit_v = torch.zeros(3, N, dtype=torch.float32, device=dev)
+            self.exit_w = torch.zeros(N, dtype=torch.float32, device=dev)
+        else:
+            self.exit_add = self.exit_p = self.exit_v = self.exit_w = None
+        if spec.photon_stats:
+            self.ph = torch.zeros(3, N, dtype=torch.int32, device=dev)
+        else:
+            self.ph = None
+
+    def zero_(self) -> "Tallies":
+        for t in (self.ledger, self.counters, self.rr, self.absorbed):
+            if t is not None:
+                t.zero_()
+        self.n_photons = 0
+        return self
+
+    def struct(self) -> A.PmoTallies:
+        sp = self.spec
+        t = A.PmoTallies()
+        t.ledger = self.ledger.data_ptr()
+        t.counters = self.counters.data_ptr()
+        t.rr = _ptr(self.rr)
+        t.nr = int(sp.nr)
+        t.dr = float(sp.dr)
+        t.fluence_mode = int(sp.fluence)
+        t.absorbed = _ptr(self.absorbed)
+        if sp.fluence == A.PMO_FLU_SHARED:
+            lo, dim = sp.window
+            for a in range(3):
+                t.win_lo[a] = int(lo[a])
+                t.win_dim[a] = int(dim[a])
+        t.exit_add, t.exit_p = _ptr(self.exit_add), _ptr(self.exit_p)
+        t.exit_v, t.exit_w = _ptr(self.exit_v), _ptr(self.exit_w)
+        if self.ph is not None:
+            t.ph_interact = self.ph[0].data_ptr()
+            t.ph_cross = self.ph[1].data_ptr()
+            t.ph_fresnel = self.ph[2].data_ptr()
+        return t
+
+    # ---- host views -------------------------------------------------------
+    def host_counters(self) -> np.ndarray:
+        return self.counters.cpu().numpy().view(np.uint64)
+
+    def check(self) -> None:
+        """Synchronise and raise if any photon ended in an error."""
+        c = np.ascontiguousarray(self.host_counters())
+        status = load().pmo_check_counters(c.ctypes.data)
+        if status != A.PMO_OK:
+            raise PmoError(status, "transport")
+
+    def summary(self) -> dict:
+        L = self.ledger.cpu().numpy()
+        c = self.host_counters()
+        n = max(self.n_photons, 1)
+        return {
+            "nPh": self.n_photons,
+            "Rd": L[A.PMO_L_RD] / n,
+            "Tt": L[A.PMO_L_TT] / n,
+            "A": L[A.PMO_L_ABS] / n,
+            "ledger": L,
+            "counters": c,
+        }
+
+
+def run_plain(dprob: DeviceProblem, n_photons: int, seed: int, *, tallies: Tallies = None,
+              spec: TallySpec = None, begin: int = 0, precision: int = A.PMO_FP32,
+              block_threads: int = 0, blocks_per_sm: int = 0, max_events: int = 0,
+              stream=None) -> Tallies:
+    """Trace photons ``[begin, begin + n_photons)`` and accumulate into
+    ``tallies`` (created when None).  Asynchronous on the current stream."""
+    lib = load()
+    if tallies is None:
+        tallies = Tallies(dprob, spec or TallySpec(), n_photons)
+    sp = tallies.spec
+    flags = (A.PMO_FLAG_EXPORT_EXITS if sp.export_exits else 0) | \
+            (A.PMO_FLAG_PHOTON_STATS if sp.photon_stats else 0)
+    if flags and n_photons > tallies.capacity:
+        raise ValueError("per-photon outputs were sized for fewer photons")
+    s = dprob.struct(seed, begin, n_photons, precision, flags, max_events)
+    t = tallies.struct()
+    launch = A.PmoLaunch(int(block_threads), int(blocks_per_sm))
+    st = lib.pmo_run_plain(C.byref(s), C.byref(t), C.byref(launch),
+                           C.c_void_p(dprob.workspace.data_ptr()),
+                           dprob.workspace.numel(), _stream_handle(stream))
+    check(st, "pmo_run_plain")
+    tallies.n_photons += int(n_photons)
+    return tallies
+
+
+def normalize_fluence(dprob: DeviceProblem, tallies: Tallies, stream=None) -> torch.Tensor:
+    """FP64 fluence of the interior voxels, phi = absorbed / (nPh * l^3 * mu_a)."""
+    if tallies.absorbed is None:
+        raise ValueError("the run did not tally fluence")
+    nx, ny, nz = dprob.labels.shape
+    phi = torch.empty((nx - 2, ny - 2, nz - 2), dtype=torch.float64, device=dprob.device)
+    s = dprob.struct(0, 0, 0, A.PMO_FP32)
+    st = load().pmo_normalize_fluence(C.byref(s), C.c_void_p(tallies.absorbed.data_ptr()),
+                                      float(max(tallies.n_photons, 1)),
+                                      C.c_void_p(phi.data_ptr()), _stream_handle(stream))
+    check(st, "pmo_normalize_fluence")
+    return phi
+
+
+def cuvmc(add: torch.Tensor, p: torch.Tensor, v: torch.Tensor, w: torch.Tensor,
+          ma: torch.Tensor, ms: torch.Tensor, n: torch.Tensor, g: torch.Tensor,
+          voxel_model: torch.Tensor, l: float, nPh: int, end_point: int, rand_seed: int,
+          workspace: torch.Tensor, stream=None) -> None:
+    """Drop-in for the reference kernel launch ``func(grid, block, (add, p, v,
+    w, ma, ms, n, g, voxel_model, l, M, L, nPh, end_point, rand_seed))``
+    (pymopt/voxel_gpu/_classes.py:105-111): updates add/p/v/w in place."""
+    lib = load()
+    K, M, L = voxel_model.shape
+    for t, dt in ((add, torch.int32), (p, torch.float32), (v, torch.float32),
+                  (w, torch.float32), (ma, torch.float32), (ms, torch.float32),
+                  (n, torch.float32), (g, torch.float32), (voxel_model, torch.int8)):
+        if t.dtype != dt or not t.is_cuda or not t.is_contiguous():
+            raise ValueError(f"cuvmc expects contiguous CUDA {dt} tensors")
+    st = lib.pmo_cuvmc(add.data_ptr(), p.data_ptr(), v.data_ptr(), w.data_ptr(),
+                       ma.data_ptr(), ms.data_ptr(), n.data_ptr(), g.data_ptr(),
+                       voxel_model.data_ptr(), float(l), int(M), int(L), int(nPh),
+                       int(end_point), int(rand_seed), int(K),
+                       C.c_void_p(workspace.data_ptr()), workspace.numel(),
+                       _stream_handle(stream))
+    check(st, "pmo_cuvmc")
