@@ -1,0 +1,398 @@
+#!/usr/bin/env python3
+"""Photon-transport benchmark on one B200 (or N replicas).
+
+Workload (one step): 1e8 photons of the three-layer skin slab — 400x400x400
+voxels at 0.05 mm (padded 402^3 uint8 labels), epidermis 0.1 mm / dermis 2 mm
+/ subcutis, collimated Gaussian beam of 1 mm 1/e^2 radius, FP32 transport,
+FP64 ledger, R(r)/T(r) with 100 bins of 0.1 mm.  Synthetic and seeded; no
+dataset is involved.
+
+``value`` is photons/s with the volume resident in HBM, timed with CUDA events
+on the launching stream, L2 flushed between steps; ``e2e`` is the same metric
+through the engine API with the label volume copied from pinned host memory
+and the tallies read back every step.  ``--impl reference`` times the CPU
+restatement of the reference algorithm (oracle/vmc_oracle.c, FP32, all host
+threads) on a bounded sample of the same workload.
+
+Multi-GPU (``torchrun --nproc-per-node N``): photons are independent, so each
+rank runs its own photon range of the same problem (weak scaling, no
+collective on the data path); only the timing uses a barrier and a MAX
+reduction.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "photons/s per B200 at R(r) within 3σ of ref"
+UNIT = "photons/s"
+WORKLOAD = "c2_three_layer_skin_400^3_gaussian_beam"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse_args():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--photons", type=float, default=1e8, help="photons per step per GPU")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--block-threads", type=int, default=0)
+    ap.add_argument("--blocks-per-sm", type=int, default=0)
+    return ap.parse_args()
+
+
+def config_dict(photons: int, world: int) -> dict:
+    from pymonteopt_b200 import volumes as V
+    return {
+        "workload": WORKLOAD,
+        "voxels": [402, 402, 402],
+        "voxel_space_mm": V.C2_PARAMS["voxel_space"],
+        "layers_mm": V.C2_PARAMS["thickness"],
+        "w_beam_mm": V.C2_W_BEAM,
+        "photons_per_step_per_gpu": photons,
+        "rr_bins": [100, 0.1],
+        "fluence_tally": False,
+        "l2": "flushed between timed steps (256 MiB write); label volume 65 MB < L2",
+        "parallelism": f"replicas x{world} (photon ranges per GPU, no collectives)",
+    }
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": num(rows[0][2]), "reasons": reasons, "samples": len(rows),
+                "power_w_max": max((num(r[3]) or 0.0) for r in rows)}
+
+
+# ---------------------------------------------------------------------------
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def cpu_oracle_rate(target_seconds: float, seed: int = 1234) -> dict:
+    """Photons/s of the FP32 CPU restatement on this host's cores, on a
+    bounded sample of the benchmark workload."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle  # noqa: E402  (test infrastructure; CPU baseline only)
+    from pymonteopt_b200 import _abi as A
+    from pymonteopt_b200 import volumes as V
+    prob = V.c2_skin()
+    threads = host_threads()
+    n = max(200, 50 * threads)
+    t0 = time.perf_counter()
+    oracle.run(prob, n, seed, precision=A.PMO_FP32, nr=100, dr=0.1, threads=threads)
+    dt = time.perf_counter() - t0
+    n2 = int(max(n, min(5e7, n * target_seconds / max(dt, 1e-3))))
+    t0 = time.perf_counter()
+    r = oracle.run(prob, n2, seed + 1, begin=n, precision=A.PMO_FP32, nr=100, dr=0.1,
+                   threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": n2 / dt, "photons": n2, "seconds": dt, "threads": threads,
+            "Rd": float(r["ledger"][A.PMO_L_RD] / n2)}
+
+
+def run_reference(args, rank: int, world: int) -> None:
+    """Reference arm: the CPU restatement of the reference transport
+    (oracle/vmc_oracle.c, FP32, all host threads) on a bounded sample of the
+    workload per step.  Under torchrun only rank 0 runs."""
+    if rank != 0:
+        return
+    photons = int(args.photons)
+    per_step = max(2.0, min(20.0, 150.0 / max(args.steps + args.warmup, 1)))
+    for _ in range(args.warmup):
+        cpu_oracle_rate(per_step / 4)
+    vals, secs, sample = [], 0.0, 0
+    for k in range(args.steps):
+        r = cpu_oracle_rate(per_step, seed=100 + k)
+        vals.append(r["value"])
+        secs += r["seconds"]
+        sample += r["photons"]
+    value = float(np.mean(vals))
+    line = {
+        "impl": "reference",
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * photons / value,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32", "data": "synthetic",
+        "config": config_dict(photons, world),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": r["threads"], "kind": "port",
+                         "sample": f"{sample} photons of the workload over {args.steps} steps "
+                                   f"({secs:.1f} s), oracle/vmc_oracle.c FP32, OpenMP"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def fp32_probe(torch, lib) -> float:
+    """Measured FP32 issue rate (FFMA thread-instructions per second)."""
+    import ctypes as C
+    props = torch.cuda.get_device_properties(torch.cuda.current_device())
+    blocks, threads = props.multi_processor_count * 8, 256
+    out = torch.zeros(blocks, dtype=torch.float32, device="cuda")
+    s = torch.cuda.current_stream()
+    iters = 2000
+    best = 0.0
+    for rep in range(4):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(s)
+        st = lib.pmo_fp32_probe(C.c_void_p(out.data_ptr()), blocks, threads, iters,
+                                C.c_void_p(s.cuda_stream))
+        e1.record(s)
+        torch.cuda.synchronize()
+        assert st == 0
+        if rep == 0:
+            continue
+        t = e0.elapsed_time(e1) / 1e3
+        best = max(best, blocks * threads * iters * 128 / t)
+    return best
+
+
+def read_traffic():
+    """DRAM bytes per photon of the transport kernel from the committed ncu
+    summary, if present."""
+    path = os.path.join(REPO, "profiles", "vmc_plain_c2_ncu.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        return json.load(f)
+
+
+def main() -> int:
+    args = parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return 0
+
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    from pymonteopt_b200 import _abi as A
+    from pymonteopt_b200 import engine as E
+    from pymonteopt_b200 import opcount
+    from pymonteopt_b200 import volumes as V
+    from pymonteopt_b200._lib import load
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+    lib = load()
+    photons = int(args.photons)
+    stream = torch.cuda.current_stream()
+
+    prob = V.c2_skin()
+    dp = E.DeviceProblem(prob, dev)
+    spec = E.TallySpec(nr=100, dr=0.1)
+    begin0 = rank * photons * (args.steps + args.warmup + 1)
+
+    def step(k: int, tallies):
+        return E.run_plain(dp, photons, seed=1000 + k, tallies=tallies,
+                           begin=begin0 + k * photons,
+                           block_threads=args.block_threads, blocks_per_sm=args.blocks_per_sm)
+
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=dev)
+    for k in range(args.warmup):
+        t = step(k, E.Tallies(dp, spec, photons))
+    torch.cuda.synchronize()
+    t.check()
+
+    peak = fp32_probe(torch, lib)
+
+    # ---- timed region: value -------------------------------------------
+    tallies = [E.Tallies(dp, spec, photons) for _ in range(args.steps)]
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    clocks = ClockSampler(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    w0 = time.perf_counter()
+    for k in range(args.steps):
+        flush.zero_()                       # L2 flush between timed steps
+        evs[k][0].record(stream)
+        step(args.warmup + k, tallies[k])
+        evs[k][1].record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    wall = time.perf_counter() - w0
+    clk = clocks.stop()
+    dev_s = sum(a.elapsed_time(b) for a, b in evs) / 1e3
+    for t in tallies:
+        t.check()
+    t_max = torch.tensor([dev_s], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+    dev_s_max = float(t_max.item())
+    total_photons = photons * args.steps * world
+    value = total_photons / dev_s_max
+
+    counters = sum(t.host_counters().astype(np.float64) for t in tallies)
+    ledger = sum(t.ledger.cpu().numpy() for t in tallies)
+    fp32_per_launch = opcount.fp32_ops(counters.astype(np.uint64)) / args.steps
+    launch_s = dev_s / args.steps
+    achieved = fp32_per_launch / launch_s
+    traffic = read_traffic()
+    roofline = {
+        "bound": "fp32-issue",
+        "achieved": achieved / 1e9, "peak": peak / 1e9, "unit": "G FP32 inst/s",
+        "frac": achieved / peak,
+        "peak_source": "measured in this run: FFMA-throughput probe (pmo_fp32_probe)",
+        "traffic": (traffic["dram_bytes_per_photon"] * photons) if traffic else None,
+        "traffic_unit": "bytes per launch (ncu dram__bytes_read+write, scaled per photon)",
+        "algorithmic_fp32_per_photon": fp32_per_launch / photons,
+        "mufu_per_photon": opcount.mufu_ops(counters.astype(np.uint64)) / (photons * args.steps),
+        "philox_draws_per_photon": opcount.philox_draws(counters.astype(np.uint64)) / (photons * args.steps),
+    }
+    inflow = ledger[A.PMO_L_WINIT] + ledger[A.PMO_L_RGAIN]
+    outflow = (ledger[A.PMO_L_RD] + ledger[A.PMO_L_TT] + ledger[A.PMO_L_EXIT0] +
+               ledger[A.PMO_L_ABS] + ledger[A.PMO_L_RLOSS] + ledger[A.PMO_L_ERRW])
+    nsteps_ph = photons * args.steps
+    results = {"Rd": ledger[A.PMO_L_RD] / nsteps_ph, "Tt": ledger[A.PMO_L_TT] / nsteps_ph,
+               "A": ledger[A.PMO_L_ABS] / nsteps_ph,
+               "energy_balance_rel": (inflow - outflow) / inflow,
+               "interactions_per_photon": counters[A.PMO_C_INTERACT] / nsteps_ph,
+               "crossings_per_photon": counters[A.PMO_C_CROSS] / nsteps_ph}
+
+    # ---- e2e: engine API with host buffers --------------------------------
+    e2e = None
+    if not args.no_e2e:
+        pinned_labels = torch.from_numpy(prob.labels).pin_memory()
+        pinned_tabs = [torch.from_numpy(a).pin_memory() for a in (prob.ma, prob.ms, prob.g, prob.n)]
+        host_ledger = torch.empty(A.PMO_LEDGER_N, dtype=torch.float64).pin_memory()
+        host_rr = torch.empty(A.PMO_RR_CATS, 100, dtype=torch.float32).pin_memory()
+        host_cnt = torch.empty(A.PMO_COUNTERS_N, dtype=torch.int64).pin_memory()
+        h2d = pinned_labels.numel() + sum(t.numel() * 4 for t in pinned_tabs)
+        d2h = host_ledger.numel() * 8 + host_rr.numel() * 4 + host_cnt.numel() * 8
+        et = E.Tallies(dp, spec, photons)
+        e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                for _ in range(args.steps)]
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        for k in range(args.steps):
+            flush.zero_()
+            e_ev[k][0].record(stream)
+            dp.labels.copy_(pinned_labels, non_blocking=True)
+            for dst, src in zip((dp.ma, dp.ms, dp.g, dp.n), pinned_tabs):
+                dst.copy_(src, non_blocking=True)
+            et.zero_()
+            E.run_plain(dp, photons, seed=5000 + k, tallies=et, begin=begin0 + k * photons,
+                        block_threads=args.block_threads, blocks_per_sm=args.blocks_per_sm)
+            host_ledger.copy_(et.ledger, non_blocking=True)
+            host_rr.copy_(et.rr, non_blocking=True)
+            host_cnt.copy_(et.counters, non_blocking=True)
+            e_ev[k][1].record(stream)
+        torch.cuda.synchronize()
+        e_s = torch.tensor([sum(a.elapsed_time(b) for a, b in e_ev) / 1e3],
+                           dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(e_s, op=dist.ReduceOp.MAX)
+        e2e = {"value": total_photons / float(e_s.item()), "unit": UNIT,
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r = cpu_oracle_rate(12.0)
+        cpu = {"value": r["value"], "unit": UNIT, "cores": r["threads"], "kind": "port",
+               "sample": f"{r['photons']} photons of the workload in {r['seconds']:.1f} s "
+                         f"(oracle/vmc_oracle.c FP32, OpenMP, {r['threads']} threads)"}
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return 0
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * dev_s_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "fp32", "data": "synthetic",
+        "config": config_dict(photons, world),
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": args.steps,
+        "clocks": clk,
+        "wall_s_timed_region": wall,
+        "results": results,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

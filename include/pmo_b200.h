@@ -109,6 +109,12 @@ typedef struct pmo_problem {
     const uint8_t *labels;
     int32_t nx, ny, nz;
     float voxel_space;           /* l [mm] */
+    /* optional uniform-box map from pmo_build_voxel_words (label in the low
+       byte, box radius in the high byte).  With it, photons in per-label
+       optics step from the face of one label-uniform cube to the next instead
+       of from voxel face to voxel face: the same path, fewer crossings.
+       NULL: voxel-by-voxel stepping exactly as the reference. */
+    const uint16_t *voxel_words;
     int32_t end_label;           /* shell label; photons leave when they enter it */
 
     /* optics: per-label tables of n_labels entries (n_labels <= 256);
@@ -230,6 +236,20 @@ int pmo_philox_words_curand(unsigned long long seed,
                             const unsigned long long *subsequence,
                             const unsigned long long *block, uint32_t *out,
                             int n, void *stream);
+
+/* FP32 issue-rate probe: blocks x threads threads each issue iters * 128
+   independent FFMA instructions.  Timed by the caller; gives the measured
+   denominator of the FP32-issue roofline.  No counterpart in the reference. */
+int pmo_fp32_probe(float *out, int blocks, int threads, int iters, void *stream);
+
+/* Uniform-box map of a label volume: words[i] = labels[i] | R << 8 where R
+   (1 .. cap+1) is the Chebyshev distance from voxel i to the nearest voxel
+   of another label (array border counted as a label change).  scratch:
+   2 * nx*ny*nz bytes of device memory.  No counterpart in the reference,
+   which steps voxel by voxel (pymopt/voxel_gpu/_cukernel.py:77-176). */
+int pmo_build_voxel_words(const uint8_t *labels, int nx, int ny, int nz, int cap,
+                          uint16_t *words, void *scratch, size_t scratch_bytes,
+                          void *stream);
 
 /* Turn device-side counters (after the caller synchronised) into a status. */
 int pmo_check_counters(const unsigned long long *host_counters);

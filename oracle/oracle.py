@@ -76,10 +76,11 @@ def _ptr(a):
 
 def run(prob, n_photons: int, seed: int, *, begin: int = 0, precision: int = A.PMO_FP64,
         nr: int = 0, dr: float = 0.1, fluence: bool = False, per_photon: bool = False,
-        threads: int = 0, max_events: int = 0) -> dict:
+        threads: int = 0, max_events: int = 0, validate: bool = True) -> dict:
     """Trace photons ``[begin, begin + n_photons)`` of ``prob`` on the CPU."""
     lib = load()
-    prob.validate()
+    if validate:
+        prob.validate()
     s = A.PmoProblem()
     prob.fill_struct(s)
     keep = [prob.labels, prob.ma, prob.ms, prob.g, prob.n]

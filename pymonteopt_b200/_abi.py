@@ -95,6 +95,7 @@ class PmoProblem(C.Structure):
         ("labels", C.c_void_p),
         ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
         ("voxel_space", C.c_float),
+        ("voxel_words", C.c_void_p),
         ("end_label", C.c_int32),
         ("props_mode", C.c_int32),
         ("n_labels", C.c_int32),

@@ -35,6 +35,9 @@ SIGNATURES = {
     "pmo_check_counters": (C.c_int, [C.c_void_p]),
     "pmo_philox_words": (C.c_int, [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_int,
                                    C.c_void_p]),
+    "pmo_build_voxel_words": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                        C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]),
+    "pmo_fp32_probe": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p]),
     "pmo_philox_words_curand": (C.c_int, [C.c_ulonglong, C.c_void_p, C.c_void_p, C.c_void_p,
                                           C.c_int, C.c_void_p]),
 }

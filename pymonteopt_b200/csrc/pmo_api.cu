@@ -87,6 +87,7 @@ int problem_to_params(const pmo_problem *p, KParams *kp) {
 
     std::memset(kp, 0, sizeof(*kp));
     kp->labels = p->labels;
+    kp->words = p->voxel_words;
     kp->nx = p->nx;
     kp->ny = p->ny;
     kp->nz = p->nz;
@@ -175,7 +176,7 @@ int tallies_to_params(const pmo_problem *p, const pmo_tallies *t, KParams *kp) {
 
 int launch_kp(const KParams &kp, int precision, int props, int flu, const pmo_launch *launch,
               cudaStream_t s) {
-    int threads = launch && launch->block_threads > 0 ? launch->block_threads : 256;
+    int threads = launch && launch->block_threads > 0 ? launch->block_threads : 128;
     if (threads % 32 != 0 || threads > 512) return PMO_ERR_ARG;
     const int bps = launch ? launch->blocks_per_sm : 0;
     cudaError_t e = cudaMemsetAsync(kp.work, 0, sizeof(unsigned long long), s);

@@ -12,6 +12,7 @@ namespace pmo {
 struct KParams {
     // geometry
     const uint8_t *labels;
+    const uint16_t *words;         // label | uniform-box radius << 8, or null
     int32_t nx, ny, nz;
     uint32_t sx, sy;               // strides of x and y in the label volume
     float l;

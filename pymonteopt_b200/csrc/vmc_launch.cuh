@@ -20,10 +20,10 @@ inline int device_sm_count() {
     return cached[dev];
 }
 
-template <typename R, int PROPS, int FLU>
+template <typename R, int PROPS, int FLU, bool SKIP>
 cudaError_t launch_plain_t(const KParams &kp, int threads, int blocks_per_sm, cudaStream_t s,
                            LaunchShape *out) {
-    auto kern = vmc_plain_kernel<R, PROPS, FLU>;
+    auto kern = vmc_plain_kernel<R, PROPS, FLU, SKIP>;
     const size_t smem = SmemLayout<R>::total(kp.nr, kp.rr_shared, FLU, kp.win_dim);
     cudaError_t e;
     if (smem > 48 * 1024) {
@@ -49,17 +49,30 @@ cudaError_t launch_plain_t(const KParams &kp, int threads, int blocks_per_sm, cu
     return cudaGetLastError();
 }
 
+template <typename R, bool SKIP>
+cudaError_t launch_plain_label(const KParams &kp, int flu, int threads, int bps, cudaStream_t s,
+                               LaunchShape *out) {
+    if (flu == PMO_FLU_NONE)
+        return launch_plain_t<R, PMO_PROPS_LABEL, PMO_FLU_NONE, SKIP>(kp, threads, bps, s, out);
+    if (flu == PMO_FLU_GLOBAL)
+        return launch_plain_t<R, PMO_PROPS_LABEL, PMO_FLU_GLOBAL, SKIP>(kp, threads, bps, s, out);
+    return launch_plain_t<R, PMO_PROPS_LABEL, PMO_FLU_SHARED, SKIP>(kp, threads, bps, s, out);
+}
+
+// Uniform-box stepping whenever a voxel-word map is given and the optics are
+// per label; per-voxel optics step voxel by voxel.
 template <typename R>
 cudaError_t launch_plain_r(const KParams &kp, int props, int flu, int threads, int bps,
                            cudaStream_t s, LaunchShape *out) {
     if (props == PMO_PROPS_LABEL) {
-        if (flu == PMO_FLU_NONE) return launch_plain_t<R, PMO_PROPS_LABEL, PMO_FLU_NONE>(kp, threads, bps, s, out);
-        if (flu == PMO_FLU_GLOBAL) return launch_plain_t<R, PMO_PROPS_LABEL, PMO_FLU_GLOBAL>(kp, threads, bps, s, out);
-        return launch_plain_t<R, PMO_PROPS_LABEL, PMO_FLU_SHARED>(kp, threads, bps, s, out);
+        if (kp.words) return launch_plain_label<R, true>(kp, flu, threads, bps, s, out);
+        return launch_plain_label<R, false>(kp, flu, threads, bps, s, out);
     }
-    if (flu == PMO_FLU_NONE) return launch_plain_t<R, PMO_PROPS_VOXEL, PMO_FLU_NONE>(kp, threads, bps, s, out);
-    if (flu == PMO_FLU_GLOBAL) return launch_plain_t<R, PMO_PROPS_VOXEL, PMO_FLU_GLOBAL>(kp, threads, bps, s, out);
-    return launch_plain_t<R, PMO_PROPS_VOXEL, PMO_FLU_SHARED>(kp, threads, bps, s, out);
+    if (flu == PMO_FLU_NONE)
+        return launch_plain_t<R, PMO_PROPS_VOXEL, PMO_FLU_NONE, false>(kp, threads, bps, s, out);
+    if (flu == PMO_FLU_GLOBAL)
+        return launch_plain_t<R, PMO_PROPS_VOXEL, PMO_FLU_GLOBAL, false>(kp, threads, bps, s, out);
+    return launch_plain_t<R, PMO_PROPS_VOXEL, PMO_FLU_SHARED, false>(kp, threads, bps, s, out);
 }
 
 }  // namespace pmo

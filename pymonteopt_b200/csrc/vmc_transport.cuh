@@ -103,7 +103,7 @@ struct SmemLayout {
 
 enum : int { kChunk = 64 };
 
-template <typename R, int PROPS, int FLU>
+template <typename R, int PROPS, int FLU, bool SKIP>
 __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using L = SmemLayout<R>;
@@ -138,6 +138,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
     const uint2 key = make_uint2(kp.key0, kp.key1);
     const R l = (R)kp.l;
     const R hl = l / 2;
+    const R inv_l = R(1) / l;
     const uint32_t cap = kp.max_events ? kp.max_events : (1u << 26);
     const uint64_t N = kp.count;
     const bool export_exits = (kp.flags & PMO_FLAG_EXPORT_EXITS) != 0;
@@ -148,12 +149,16 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
     unsigned long long t_int = 0, t_cross = 0;
     uint32_t t_fres = 0, t_refl = 0, t_roul = 0, t_same = 0;
 
-    // photon state (registers)
+    // photon state (registers).  The photon sits in a label-uniform box of
+    // (2 rad - 1)^3 voxels centred on voxel (ix, iy, iz) with linear index
+    // lin; (px, py, pz) is its offset from that voxel's centre and hw the
+    // box half-width.  rad == 1 is the reference's voxel-by-voxel stepping.
     uint64_t j = 0;
     uint32_t idlo = 0, idhi = 0;
-    int ix = 0, iy = 0, iz = 0, lab = 0;
+    int ix = 0, iy = 0, iz = 0, lab = 0, rad = 1;
     uint32_t lin = 0;
     R px = 0, py = 0, pz = 0, vx = 0, vy = 0, vz = 0, ivx = 0, ivy = 0, ivz = 0, w = 0;
+    R hw = 0;
     R mt = 0, imt = 0, ma_mt = 0, ni = 1;
     uint32_t k = 0, f = 0, ncr = 0, ev = 0;
     uint32_t pend_lin = 0xffffffffu;
@@ -164,22 +169,43 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
         pend_w = 0.f;
         pend_lin = 0xffffffffu;
     };
+    // offset of the voxel holding the photon from the box centre, in voxels
+    auto box_k = [&](R q) -> int {
+        const int m = rad - 1;
+        int k = (int)rint(q * inv_l);
+        return k < -m ? -m : (k > m ? m : k);
+    };
     auto deposit = [&](float dw) {
+        int cx = ix, cy = iy, cz = iz;
+        uint32_t clin = lin;
+        if (SKIP && rad > 1) {
+            const int kx = box_k(px), ky = box_k(py), kz = box_k(pz);
+            // a map from pmo_build_voxel_words keeps every box inside the
+            // array; a caller-supplied map that does not loses the deposit
+            // to the box centre instead of writing outside the grid
+            if ((unsigned)(cx + kx) < (unsigned)kp.nx && (unsigned)(cy + ky) < (unsigned)kp.ny &&
+                (unsigned)(cz + kz) < (unsigned)kp.nz) {
+                cx += kx;
+                cy += ky;
+                cz += kz;
+                clin += (uint32_t)kx * kp.sx + (uint32_t)ky * kp.sy + (uint32_t)kz;
+            }
+        }
         if (FLU == PMO_FLU_SHARED) {
-            const unsigned wx = (unsigned)(ix - kp.win_lo[0]);
-            const unsigned wy = (unsigned)(iy - kp.win_lo[1]);
-            const unsigned wz = (unsigned)(iz - kp.win_lo[2]);
+            const unsigned wx = (unsigned)(cx - kp.win_lo[0]);
+            const unsigned wy = (unsigned)(cy - kp.win_lo[1]);
+            const unsigned wz = (unsigned)(cz - kp.win_lo[2]);
             if (wx < (unsigned)kp.win_dim[0] && wy < (unsigned)kp.win_dim[1] &&
                 wz < (unsigned)kp.win_dim[2]) {
                 atomicAdd(s_win + ((wx * kp.win_dim[1] + wy) * kp.win_dim[2] + wz), dw);
                 return;
             }
         }
-        if (lin == pend_lin) {
+        if (clin == pend_lin) {
             pend_w += dw;
         } else {
             deposit_flush();
-            pend_lin = lin;
+            pend_lin = clin;
             pend_w = dw;
         }
     };
@@ -334,7 +360,15 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             return false;
         }
         lin = ((uint32_t)ix * (uint32_t)kp.ny + (uint32_t)iy) * (uint32_t)kp.nz + (uint32_t)iz;
-        lab = __ldg(kp.labels + lin);
+        if (SKIP) {
+            const uint32_t word = __ldg(kp.words + lin);
+            lab = (int)(word & 0xffu);
+            rad = (int)(word >> 8);
+        } else {
+            lab = __ldg(kp.labels + lin);
+            rad = 1;
+        }
+        hw = (R)rad * l - hl;
         if (!s_valid[lab]) {
             fail(PMO_C_ERR_LABEL);
             return false;
@@ -355,9 +389,9 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
 
         for (;;) {
             // distance to the nearest face; db starts at 1000 (:80-90)
-            const R dx = (copysign(hl, vx) - px) * ivx;
-            const R dy = (copysign(hl, vy) - py) * ivy;
-            const R dz = (copysign(hl, vz) - pz) * ivz;
+            const R dx = (copysign(hw, vx) - px) * ivx;
+            const R dy = (copysign(hw, vy) - py) * ivy;
+            const R dz = (copysign(hw, vz) - pz) * ivz;
             R db = R(1000);
             int ax = 0;
             if (dx < db) { db = dx; ax = 0; }
@@ -377,7 +411,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             py += vy * db;
             pz += vz * db;
             const R va = ax == 0 ? vx : (ax == 1 ? vy : vz);
-            const R face = copysign(hl, va);
+            const R face = copysign(hw, va);
             if (ax == 0) px = face;
             else if (ax == 1) py = face;
             else pz = face;
@@ -385,19 +419,58 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             ++ncr;
             if (++ev > cap) { fail(PMO_C_ERR_CAP); return false; }
             const bool neg = signbit(va);
-            const int cc = ax == 0 ? ix : (ax == 1 ? iy : iz);
+            // the voxel of the box that touches this face, and the photon's
+            // offset inside it (for rad == 1: the box itself)
+            int cx = ix, cy = iy, cz = iz;
+            uint32_t clin = lin;
+            R fx = px, fy = py, fz = pz;
+            if (SKIP && rad > 1) {
+                const int m = neg ? -(rad - 1) : rad - 1;
+                const int kx = ax == 0 ? m : box_k(px);
+                const int ky = ax == 1 ? m : box_k(py);
+                const int kz = ax == 2 ? m : box_k(pz);
+                fx = ax == 0 ? copysign(hl, va) : px - (R)kx * l;
+                fy = ax == 1 ? copysign(hl, va) : py - (R)ky * l;
+                fz = ax == 2 ? copysign(hl, va) : pz - (R)kz * l;
+                cx += kx;
+                cy += ky;
+                cz += kz;
+                clin += (uint32_t)kx * kp.sx + (uint32_t)ky * kp.sy + (uint32_t)kz;
+                if ((unsigned)cx >= (unsigned)kp.nx || (unsigned)cy >= (unsigned)kp.ny ||
+                    (unsigned)cz >= (unsigned)kp.nz) {
+                    fail(PMO_C_ERR_GEOM);  // only a malformed caller-supplied map
+                    return false;
+                }
+            }
+            const int cc = ax == 0 ? cx : (ax == 1 ? cy : cz);
             const int dim = ax == 0 ? kp.nx : (ax == 1 ? kp.ny : kp.nz);
             const int nc = neg ? cc - 1 : cc + 1;
             if ((unsigned)nc >= (unsigned)dim) { fail(PMO_C_ERR_GEOM); return false; }
             const uint32_t stride = ax == 0 ? kp.sx : (ax == 1 ? kp.sy : 1u);
-            const uint32_t nlin = neg ? lin - stride : lin + stride;
-            const int nlab = __ldg(kp.labels + nlin);
+            const uint32_t nlin = neg ? clin - stride : clin + stride;
+            int nlab, nrad = 1;
+            if (SKIP) {
+                const uint32_t word = __ldg(kp.words + nlin);
+                nlab = (int)(word & 0xffu);
+                nrad = (int)(word >> 8);
+            } else {
+                nlab = __ldg(kp.labels + nlin);
+            }
+            // step into the neighbour voxel and take its box (:137-148)
+            auto enter = [&]() {
+                ix = ax == 0 ? nc : cx;
+                iy = ax == 1 ? nc : cy;
+                iz = ax == 2 ? nc : cz;
+                px = ax == 0 ? -fx : fx;
+                py = ax == 1 ? -fy : fy;
+                pz = ax == 2 ? -fz : fz;
+                lin = nlin;
+                rad = nrad;
+                hw = (R)rad * l - hl;
+            };
             if (PROPS == PMO_PROPS_LABEL && nlab == lab) {
                 // same label on the other side: same n and mu (:154-167)
-                if (ax == 0) { ix = nc; px = -px; }
-                else if (ax == 1) { iy = nc; py = -py; }
-                else { iz = nc; pz = -pz; }
-                lin = nlin;
+                enter();
                 ++t_same;
                 continue;
             }
@@ -448,10 +521,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
                 set_dir_inverse();
             }
             // cross (:137-148)
-            if (ax == 0) { ix = nc; px = -px; }
-            else if (ax == 1) { iy = nc; py = -py; }
-            else { iz = nc; pz = -pz; }
-            lin = nlin;
+            enter();
             lab = nlab;
             ni = nt;
             if (lab == kp.end_label) {

@@ -37,16 +37,30 @@ def require_cuda(device=None) -> torch.device:
     return d
 
 
-class DeviceProblem:
-    """A problem whose volume and optical tables are resident on one GPU."""
+SKIP_CAP = 31   # uniform boxes of up to (2*32 - 1)^3 voxels
 
-    def __init__(self, prob, device=None):
+
+class DeviceProblem:
+    """A problem whose volume and optical tables are resident on one GPU.
+
+    ``skip`` builds the uniform-box map (``pmo_build_voxel_words``) so that
+    photons in per-label optics step from box face to box face; the path is
+    the same as voxel-by-voxel stepping up to rounding.  ``skip=False`` keeps
+    the reference's voxel-by-voxel stepping (the FP64 oracle comparisons use
+    it)."""
+
+    def __init__(self, prob, device=None, *, skip: bool = True, skip_cap: int = SKIP_CAP):
         load()
         self.device = require_cuda(device)
         prob.validate()
         self.host = prob
         dev = self.device
         self.labels = torch.from_numpy(prob.labels).to(dev)
+        self.words = None
+        self.skip_cap = int(skip_cap)
+        if skip and prob.vox_ma is None:
+            self.words = torch.empty(prob.labels.shape, dtype=torch.int16, device=dev)
+            self.build_words()
         self.ma = torch.from_numpy(prob.ma).to(dev)
         self.ms = torch.from_numpy(prob.ms).to(dev)
         self.g = torch.from_numpy(prob.g).to(dev)
@@ -57,6 +71,15 @@ class DeviceProblem:
             self.vox_ms = torch.from_numpy(prob.vox_ms).to(dev)
         self.workspace = torch.empty(int(load().pmo_workspace_bytes()), dtype=torch.uint8,
                                      device=dev)
+
+    def build_words(self, stream=None) -> None:
+        """(Re)build the uniform-box map from the resident labels."""
+        scratch = torch.empty(2 * self.labels.numel(), dtype=torch.uint8, device=self.device)
+        nx, ny, nz = self.labels.shape
+        st = load().pmo_build_voxel_words(self.labels.data_ptr(), nx, ny, nz, self.skip_cap,
+                                          self.words.data_ptr(), scratch.data_ptr(),
+                                          scratch.numel(), _stream_handle(stream))
+        check(st, "pmo_build_voxel_words")
 
     def set_optics(self, ma=None, ms=None, vox_ma=None, vox_ms=None) -> None:
         """Replace optical properties in place (same shapes)."""
@@ -72,6 +95,7 @@ class DeviceProblem:
         s = A.PmoProblem()
         self.host.fill_struct(s)
         s.labels = self.labels.data_ptr()
+        s.voxel_words = self.words.data_ptr() if self.words is not None else None
         s.ma, s.ms, s.g, s.n = (t.data_ptr() for t in (self.ma, self.ms, self.g, self.n))
         if self.vox_ma is not None:
             s.vox_ma, s.vox_ms = self.vox_ma.data_ptr(), self.vox_ms.data_ptr()

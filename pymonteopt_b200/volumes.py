@@ -89,7 +89,7 @@ def gaussian_random_field(shape, corr_vox: float, rng: np.random.Generator) -> n
     f *= np.exp(-s2 * kx[:, None, None] ** 2)
     f *= np.exp(-s2 * ky[None, :, None] ** 2)
     f *= np.exp(-s2 * kz[None, None, :] ** 2)
-    return np.fft.irfftn(f, s=shape).astype(np.float32)
+    return np.fft.irfftn(f, s=shape, axes=(0, 1, 2)).astype(np.float32)
 
 
 C3_CLASSES = ("air", "fat", "soft tissue", "muscle", "bone")

@@ -1,0 +1,87 @@
+"""The C ABI without a GPU: header constants, struct layouts, exported symbols."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import pytest
+
+from pymonteopt_b200 import _abi as A
+from pymonteopt_b200 import _lib
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(REPO, "include", "pmo_b200.h")
+
+
+def _header():
+    with open(HEADER) as f:
+        return f.read()
+
+
+def test_header_defines_match_python():
+    defs = dict(re.findall(r"#define\s+(PMO_\w+)\s+(\d+)u?\b", _header()))
+    assert defs, "no #defines parsed"
+    for name, val in defs.items():
+        assert hasattr(A, name), f"{name} missing from _abi.py"
+        assert getattr(A, name) == int(val), name
+
+
+def _declared_functions():
+    return set(re.findall(r"^\s*(?:int|size_t|const char \*)\s*(pmo_\w+)\(", _header(), re.M))
+
+
+@pytest.fixture(scope="module")
+def built_lib():
+    from pymonteopt_b200 import _build
+    _build.build()
+    return _lib.load()
+
+
+def test_library_loads_and_exports_every_declared_symbol(built_lib):
+    names = _declared_functions()
+    assert {"pmo_run_plain", "pmo_cuvmc", "pmo_status_string"} <= names
+    for n in names:
+        assert hasattr(built_lib, n), n
+        assert n in _lib.SIGNATURES, f"{n} has no ctypes signature"
+    # entry points that need no GPU
+    assert built_lib.pmo_abi_version() == A.PMO_ABI_VERSION
+    assert built_lib.pmo_workspace_bytes() >= 512
+    assert built_lib.pmo_status_string(A.PMO_ERR_LABEL).decode().startswith("photon")
+    c = (C.c_ulonglong * A.PMO_COUNTERS_N)()
+    assert built_lib.pmo_check_counters(c) == A.PMO_OK
+    c[A.PMO_C_ERR_CAP] = 1
+    assert built_lib.pmo_check_counters(c) == A.PMO_ERR_STEP_CAP
+
+
+def test_argument_validation_rejects_before_any_device_call(built_lib):
+    # null problem / tallies are refused on the host, no CUDA call is made
+    assert built_lib.pmo_run_plain(None, None, None, None, 0, None) == A.PMO_ERR_ARG
+    p = A.PmoProblem()
+    assert built_lib.pmo_run_plain(C.byref(p), None, None, None, 0, None) == A.PMO_ERR_ARG
+
+
+def _c_offsets(struct_name, fields):
+    src = ["#include <stdio.h>", "#include <stddef.h>", f'#include "{HEADER}"', "int main(void){",
+           f'printf("%zu\\n", sizeof({struct_name}));']
+    for f in fields:
+        src.append(f'printf("%zu\\n", offsetof({struct_name}, {f}));')
+    src.append("return 0;}")
+    d = os.path.join(REPO, "oracle", "_build")
+    os.makedirs(d, exist_ok=True)
+    c_path = os.path.join(d, f"layout_{struct_name}.c")
+    exe = c_path[:-2]
+    with open(c_path, "w") as fh:
+        fh.write("\n".join(src))
+    subprocess.run(["gcc", "-o", exe, c_path], check=True)
+    out = subprocess.run([exe], check=True, capture_output=True, text=True).stdout.split()
+    return [int(x) for x in out]
+
+
+@pytest.mark.parametrize("cls,name", [(A.PmoProblem, "pmo_problem"), (A.PmoTallies, "pmo_tallies"),
+                                      (A.PmoLaunch, "pmo_launch")])
+def test_struct_layout_matches_header(cls, name):
+    fields = [f[0] for f in cls._fields_]
+    got = _c_offsets(name, fields)
+    assert got[0] == C.sizeof(cls)
+    for f, off in zip(fields, got[1:]):
+        assert getattr(cls, f).offset == off, f

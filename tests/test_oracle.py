@@ -1,0 +1,155 @@
+"""The CPU oracle pinned against the reference (CPU only).
+
+The oracle (oracle/vmc_oracle.c) restates the reference transport with a
+different random-number generator, so it is compared statistically with the
+reference's own outputs: per-seed Rd/Tt/R(r) fixtures produced by running the
+reference Numba kernel (tests/golden/make_golden.py) and the values printed in
+the reference's notebooks (tests/golden/notebook_kat.json).
+"""
+import numpy as np
+import pytest
+from scipy import stats
+
+import oracle
+from helpers import annulus_area, golden, mean_se, profile_agreement, z_score
+from pymonteopt_b200 import _abi as A
+from pymonteopt_b200 import volumes as V
+from pymonteopt_b200.problem import pencil_problem
+
+
+def _seed_batches(prob, seeds, n_per, nr, dr, precision=A.PMO_FP32):
+    area = annulus_area(nr, dr)
+    Rd, Tt, Rr, Tr = [], [], [], []
+    for s in seeds:
+        r = oracle.run(prob, n_per, s, precision=precision, nr=nr, dr=dr)
+        assert r["status"] == 0
+        L, rr = r["ledger"], r["rr"]
+        Rd.append(L[A.PMO_L_RD] / n_per)
+        Tt.append(L[A.PMO_L_TT] / n_per)
+        Rr.append((rr[A.PMO_RR_TOP] + rr[A.PMO_RR_LAT_NEG]) / (area * n_per))
+        Tr.append((rr[A.PMO_RR_BOTTOM] + rr[A.PMO_RR_LAT_POS]) / (area * n_per))
+    return Rd, Tt, Rr, Tr
+
+
+def _problem(case, g):
+    if case == "c1":
+        return V.c1_slab()
+    if case == "c2_pencil":
+        return V.c2_skin(gaussian=False)
+    if case == "c3":
+        return V.c3_ct_like(g["volume_seed"])
+    return V.plate_problem(g["params"])
+
+
+@pytest.mark.parametrize("case,n_per,precision", [
+    ("c1", 20000, A.PMO_FP32), ("c1", 20000, A.PMO_FP64),
+    ("thin_slab", 20000, A.PMO_FP32), ("semi_inf_mismatch", 20000, A.PMO_FP32),
+    ("three_layer", 20000, A.PMO_FP32), ("c2_pencil", 2000, A.PMO_FP32),
+    ("c3", 2000, A.PMO_FP32)])
+def test_oracle_matches_reference_fixtures(case, n_per, precision):
+    g = golden(f"ref_{case}.json")
+    prob = _problem(case, g)
+    Rd, Tt, Rr, Tr = _seed_batches(prob, range(200, 210), n_per, g["nr"], g["dr"], precision)
+    for mine, ref in ((Rd, g["Rd"]), (Tt, g["Tt"])):
+        m, s = mean_se(mine)
+        rm, rs = mean_se(ref)
+        if rm == 0 and rs == 0:
+            assert m < 1e-6
+            continue
+        assert abs(z_score(m, s, rm, rs)) < 3, (case, m, s, rm, rs)
+    for mine, ref in ((Rr, g["Rr"]), (Tr, g["Tr"])):
+        m, s = mean_se(mine)
+        z, chi2, dof = profile_agreement(m, s, ref)
+        if dof:
+            assert stats.chi2.sf(chi2, dof) > 1e-3, (case, chi2, dof)
+            assert np.max(np.abs(z)) < 4.5, (case, np.round(z, 2))
+
+
+def test_oracle_matches_notebook_values():
+    """Values printed by the reference notebooks (tests/golden/notebook_kat.json)."""
+    kat = golden("notebook_kat.json")
+    for case in kat["cases"]:
+        prob = V.plate_problem(case["params"])
+        n = case["oracle_photons"]
+        r = oracle.run(prob, n, 7, precision=A.PMO_FP32)
+        for key in ("Rd", "Tt"):
+            if key not in case:
+                continue
+            ref, ref_se = case[key], case.get(key + "_se")
+            mine = r["ledger"][A.PMO_L_RD if key == "Rd" else A.PMO_L_TT] / n
+            # oracle SE from the binomial-like spread of per-photon weights
+            se = max(np.sqrt(max(mine * (1 - mine), 1e-12) / n), 1e-6)
+            if ref_se is None:   # single reference run of case["ref_photons"]
+                ref_se = np.sqrt(max(ref * (1 - ref), 1e-12) / case["ref_photons"])
+            z = (mine - ref) / np.hypot(se, ref_se)
+            assert abs(z) < 3, (case["name"], key, mine, ref, z)
+
+
+@pytest.mark.parametrize("precision", [A.PMO_FP32, A.PMO_FP64])
+def test_oracle_energy_ledger(precision):
+    prob = V.plate_problem(golden("ref_three_layer.json")["params"])
+    r = oracle.run(prob, 20000, 1, precision=precision, fluence=True)
+    L = r["ledger"]
+    inflow = L[A.PMO_L_WINIT] + L[A.PMO_L_RGAIN]
+    outflow = (L[A.PMO_L_RD] + L[A.PMO_L_TT] + L[A.PMO_L_EXIT0] + L[A.PMO_L_ABS] +
+               L[A.PMO_L_RLOSS] + L[A.PMO_L_ERRW])
+    assert abs(inflow - outflow) / inflow < 1e-9
+    assert abs(r["absorbed"].sum() - L[A.PMO_L_ABS]) < 1e-9 * L[A.PMO_L_ABS]
+
+
+def test_oracle_fp32_and_fp64_share_histories():
+    prob = V.c1_slab()
+    a = oracle.run(prob, 2000, 3, precision=A.PMO_FP32, per_photon=True)
+    b = oracle.run(prob, 2000, 3, precision=A.PMO_FP64, per_photon=True)
+    same = np.all(a["ph_counts"] == b["ph_counts"], axis=1).mean()
+    assert same > 0.6
+
+
+def test_oracle_photon_ranges_compose():
+    """Photon p's history depends only on (seed, p): [0,n) == [0,k) + [k,n)."""
+    prob = V.c1_slab()
+    full = oracle.run(prob, 3000, 9, precision=A.PMO_FP64, per_photon=True)
+    a = oracle.run(prob, 1000, 9, precision=A.PMO_FP64, per_photon=True)
+    b = oracle.run(prob, 2000, 9, begin=1000, precision=A.PMO_FP64, per_photon=True)
+    assert np.array_equal(full["ph_state"], np.concatenate([a["ph_state"], b["ph_state"]]))
+    assert np.array_equal(full["ph_counts"], np.concatenate([a["ph_counts"], b["ph_counts"]]))
+
+
+def test_oracle_reports_geometry_and_label_errors():
+    vol, end = V.plate_volume(1.0, 1.0, 0.1, [0.5])
+    bad = vol.copy()
+    bad[5, 5, 2:5] = 7     # labels with no optics under the beam
+    prob = pencil_problem(bad, 0.1, end, [0.1], [10.0], [0.9], [1.37, 1.0])
+    with pytest.raises(ValueError):
+        prob.validate()    # the host check refuses the volume ...
+    r = oracle.run(prob, 500, 1, validate=False)   # ... the transport flags it too
+    assert r["counters"][A.PMO_C_ERR_LABEL] > 0
+    assert r["status"] == A.PMO_ERR_LABEL
+    hole = vol.copy()
+    hole[0, :, :] = 0      # shell missing on one face: photons walk off the array
+    prob = pencil_problem(hole, 0.1, end, [0.01], [10.0], [0.9], [1.0, 1.0])
+    with pytest.raises(ValueError):
+        prob.validate()
+    r = oracle.run(prob, 2000, 1, validate=False)
+    assert r["counters"][A.PMO_C_ERR_GEOM] > 0
+
+
+def test_philox_oracle_structure():
+    """Counter-based: the same (counter, key) gives the same words; a one-bit
+    change of the counter or key changes about half of the 128 output bits."""
+    rng = np.random.default_rng(0)
+    ctr = rng.integers(0, 2**32, size=(512, 4), dtype=np.uint64).astype(np.uint32)
+    key = (123, 456)
+    a = oracle.philox(ctr, key)
+    assert np.array_equal(a, oracle.philox(ctr, key))
+    c2 = ctr.copy()
+    c2[:, 0] ^= 1
+    flips = np.unpackbits((a ^ oracle.philox(c2, key)).view(np.uint8)).reshape(512, -1).sum(1)
+    assert 50 < flips.mean() < 78
+    k2 = oracle.philox(ctr, (123 ^ 1, 456))
+    flips = np.unpackbits((a ^ k2).view(np.uint8)).reshape(512, -1).sum(1)
+    assert 50 < flips.mean() < 78
+    # uniforms in (0, 1]
+    u = ((a.astype(np.uint64) >> 8) + 1) / 2.0 ** 24
+    assert u.min() > 0 and u.max() <= 1
+    assert abs(u.mean() - 0.5) < 0.01
