@@ -90,7 +90,7 @@ extern "C" {
 #define PMO_C_ERR_LABEL  8
 #define PMO_C_ERR_CAP    9
 #define PMO_C_ERR_NUM    10
-#define PMO_C_SAMECROSS  11      /* crossings into a voxel of the same label     */
+#define PMO_C_SAMECROSS  11      /* same-label crossings (counted by the oracle)  */
 #define PMO_COUNTERS_N   16
 
 /* ---- R(r) / T(r) histogram categories, layout [PMO_RR_CATS][nr] --------- */

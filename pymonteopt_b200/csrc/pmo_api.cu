@@ -94,6 +94,8 @@ int problem_to_params(const pmo_problem *p, KParams *kp) {
     kp->sx = (uint32_t)p->ny * (uint32_t)p->nz;
     kp->sy = (uint32_t)p->nz;
     kp->l = p->voxel_space;
+    kp->hl = p->voxel_space * 0.5f;
+    kp->inv_l = 1.0f / p->voxel_space;
     kp->end_label = p->end_label;
     kp->n_labels = p->n_labels;
     kp->ma = p->ma;

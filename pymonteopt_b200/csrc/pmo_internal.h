@@ -15,7 +15,7 @@ struct KParams {
     const uint16_t *words;         // label | uniform-box radius << 8, or null
     int32_t nx, ny, nz;
     uint32_t sx, sy;               // strides of x and y in the label volume
-    float l;
+    float l, hl, inv_l;            // voxel size, l/2, 1/l
     int32_t end_label;
     int32_t n_labels;
     // optics

@@ -137,8 +137,8 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
     const unsigned lane = threadIdx.x & 31u;
     const uint2 key = make_uint2(kp.key0, kp.key1);
     const R l = (R)kp.l;
-    const R hl = l / 2;
-    const R inv_l = R(1) / l;
+    const R hl = (R)kp.hl;
+    const R inv_l = (R)kp.inv_l;
     const uint32_t cap = kp.max_events ? kp.max_events : (1u << 26);
     const uint64_t N = kp.count;
     const bool export_exits = (kp.flags & PMO_FLAG_EXPORT_EXITS) != 0;
@@ -146,21 +146,18 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
 
     // thread totals, reduced once at the end
     double t_abs = 0.0;
-    unsigned long long t_int = 0, t_cross = 0;
-    uint32_t t_fres = 0, t_refl = 0, t_roul = 0, t_same = 0;
 
     // photon state (registers).  The photon sits in a label-uniform box of
     // (2 rad - 1)^3 voxels centred on voxel (ix, iy, iz) with linear index
     // lin; (px, py, pz) is its offset from that voxel's centre and hw the
     // box half-width.  rad == 1 is the reference's voxel-by-voxel stepping.
-    uint64_t j = 0;
-    uint32_t idlo = 0, idhi = 0;
+    uint64_t pid = 0;
     int ix = 0, iy = 0, iz = 0, lab = 0, rad = 1;
     uint32_t lin = 0;
     R px = 0, py = 0, pz = 0, vx = 0, vy = 0, vz = 0, ivx = 0, ivy = 0, ivz = 0, w = 0;
     R hw = 0;
     R mt = 0, imt = 0, ma_mt = 0, ni = 1;
-    uint32_t k = 0, f = 0, ncr = 0, ev = 0;
+    uint32_t k = 0, f = 0, ncr = 0;
     uint32_t pend_lin = 0xffffffffu;
     float pend_w = 0.f;
 
@@ -229,6 +226,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
     // photon end: per-photon outputs and counters
     auto finish = [&]() {
         if (FLU != PMO_FLU_NONE) deposit_flush();
+        const uint64_t j = pid - kp.begin;
         if (export_exits) {
             kp.exit_add[j] = ix;
             kp.exit_add[N + j] = iy;
@@ -246,9 +244,9 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             kp.ph_cross[j] = ncr;
             kp.ph_fresnel[j] = f;
         }
-        t_int += k;
-        t_cross += ncr;
-        t_fres += f;
+        atomicAdd(s_cnt + PMO_C_INTERACT, (unsigned long long)k);
+        atomicAdd(s_cnt + PMO_C_CROSS, (unsigned long long)ncr);
+        if (f) atomicAdd(s_cnt + PMO_C_FRESNEL, (unsigned long long)f);
         atomicAdd(s_cnt + PMO_C_PHOTONS, 1ull);
     };
     auto fail = [&](int counter) {
@@ -292,11 +290,8 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
     // Start photon j: source (pymopt/voxel_gpu/_classes.py:148-254).
     // Returns true when the photon is in flight.
     auto start = [&](uint64_t jj) -> bool {
-        j = jj;
-        const uint64_t pid = kp.begin + jj;
-        idlo = (uint32_t)pid;
-        idhi = (uint32_t)(pid >> 32);
-        k = f = ncr = ev = 0;
+        pid = kp.begin + jj;
+        k = f = ncr = 0;
         if (kp.source == PMO_SRC_STATE) {
             ix = kp.state_add[jj];
             iy = kp.state_add[N + jj];
@@ -320,7 +315,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             vz = (R)kp.src_v[2];
             w = (R)kp.src_w0;
             if (kp.source == PMO_SRC_GAUSSIAN || kp.spec_prob > 0.f) {
-                const uint4 rs = philox4x32_10(make_uint4(0u, 2u, idlo, idhi), key);
+                const uint4 rs = philox4x32_10(make_uint4(0u, 2u, (uint32_t)pid, (uint32_t)(pid >> 32)), key);
                 if (kp.source == PMO_SRC_GAUSSIAN) {
                     // x, y ~ N(0, sigma) (gaussianBeam, :267-287) by Box-Muller,
                     // split into voxel index + offset in [-l/2, l/2] (:242-252)
@@ -383,7 +378,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
     // faces until the step is spent, then absorb, roulette and scatter.
     // Returns true while the photon stays in flight.
     auto cycle = [&]() -> bool {
-        const uint4 rn = philox4x32_10(make_uint4(k, 0u, idlo, idhi), key);
+        const uint4 rn = philox4x32_10(make_uint4(k, 0u, (uint32_t)pid, (uint32_t)(pid >> 32)), key);
         ++k;
         R st = -plog(u01<R>(rn.x));  // step in optical depths (:75)
 
@@ -417,7 +412,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             else pz = face;
             st -= dbmt;
             ++ncr;
-            if (++ev > cap) { fail(PMO_C_ERR_CAP); return false; }
+            if (ncr + k - 1 > cap) { fail(PMO_C_ERR_CAP); return false; }
             const bool neg = signbit(va);
             // the voxel of the box that touches this face, and the photon's
             // offset inside it (for rad == 1: the box itself)
@@ -471,7 +466,6 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             if (PROPS == PMO_PROPS_LABEL && nlab == lab) {
                 // same label on the other side: same n and mu (:154-167)
                 enter();
-                ++t_same;
                 continue;
             }
             if (nlab != kp.end_label && !s_valid[nlab]) { fail(PMO_C_ERR_LABEL); return false; }
@@ -479,7 +473,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             if (ni != nt) {
                 // Fresnel / total internal reflection (:105-153) with the
                 // cosines and sines of the incidence/transmission angles
-                const uint4 fr = philox4x32_10(make_uint4(f, 1u, idlo, idhi), key);
+                const uint4 fr = philox4x32_10(make_uint4(f, 1u, (uint32_t)pid, (uint32_t)(pid >> 32)), key);
                 ++f;
                 const R u = u01<R>(fr.x);
                 R ca = fabs(va);
@@ -507,7 +501,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
                     if (ax == 0) { vx = -vx; ivx = -ivx; }
                     else if (ax == 1) { vy = -vy; ivy = -ivy; }
                     else { vz = -vz; ivz = -ivz; }
-                    ++t_refl;
+                    atomicAdd(s_cnt + PMO_C_REFLECT, 1ull);
                     continue;
                 }
                 // refract: tangential * ni/nt, normal = sign * cos(at) (:124-134)
@@ -542,7 +536,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
         }
         // Russian roulette (:182-195)
         if (w <= R(0.0001)) {
-            ++t_roul;
+            atomicAdd(s_cnt + PMO_C_ROULETTE, 1ull);
             if (R(0.1) < u01<R>(rn.y)) {
                 atomicAdd(s_led + PMO_L_RLOSS, (double)w);
                 w = R(0);
@@ -582,7 +576,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             vz *= inv;
             set_dir_inverse();
         }
-        if (++ev > cap) { fail(PMO_C_ERR_CAP); return false; }
+        if (ncr + k > cap) { fail(PMO_C_ERR_CAP); return false; }
         return true;
     };
 
@@ -621,21 +615,9 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         t_abs += __shfl_xor_sync(FULL, t_abs, o);
-        t_int += __shfl_xor_sync(FULL, t_int, o);
-        t_cross += __shfl_xor_sync(FULL, t_cross, o);
-        t_fres += __shfl_xor_sync(FULL, t_fres, o);
-        t_refl += __shfl_xor_sync(FULL, t_refl, o);
-        t_roul += __shfl_xor_sync(FULL, t_roul, o);
-        t_same += __shfl_xor_sync(FULL, t_same, o);
     }
     if (lane == 0) {
         atomicAdd(s_led + PMO_L_ABS, t_abs);
-        atomicAdd(s_cnt + PMO_C_INTERACT, (unsigned long long)t_int);
-        atomicAdd(s_cnt + PMO_C_CROSS, (unsigned long long)t_cross);
-        atomicAdd(s_cnt + PMO_C_FRESNEL, (unsigned long long)t_fres);
-        atomicAdd(s_cnt + PMO_C_REFLECT, (unsigned long long)t_refl);
-        atomicAdd(s_cnt + PMO_C_ROULETTE, (unsigned long long)t_roul);
-        atomicAdd(s_cnt + PMO_C_SAMECROSS, (unsigned long long)t_same);
     }
     __syncthreads();
     for (int i = threadIdx.x; i < PMO_LEDGER_N; i += blockDim.x)

@@ -207,15 +207,7 @@ class TuringModel_Rectangular(VoxelModel):
     _names = ["_space", "_trabecular", "_cortical", "_subcutaneus", "_dermis"]
 
     def __init__(self):
-        self.model_name = "TuringModel_Rectangular"
-        self.dtype_f = np.float32
-        self.dtype = np.int8
-        self.ct_num = 2
-        self.subc_num = 3
-        self.skin_num = 4
-        self.end_point = 5
-        self.voxel_model = np.zeros((3, 3, 3), dtype=self.dtype)
-        self.params = {
+        self._init_model("TuringModel_Rectangular", {
             "xz_size": 17.15, "voxel_space": 0.0245, "dicom_path": False, "bv_tv": 0.138,
             "th_cortical": 1., "th_subcutaneus": 2.6, "th_dermis": 1.4,
             "n_space": 1., "n_trabecular": 1.4, "n_cortical": 1.4, "n_subcutaneus": 1.4,
@@ -226,7 +218,20 @@ class TuringModel_Rectangular(VoxelModel):
             "ms_subcutaneus": 20, "ms_dermis": 20,
             "g_space": 0.90, "g_trabecular": 0.90, "g_cortical": 0.90, "g_subcutaneus": 0.90,
             "g_dermis": .90,
-        }
+        }, end_point=5)
+
+    def _init_model(self, name, params, end_point, air_num=None):
+        self.model_name = name
+        self.dtype_f = np.float32
+        self.dtype = np.int8
+        self.ct_num = 2
+        self.subc_num = 3
+        self.skin_num = 4
+        if air_num is not None:
+            self.air_num = air_num
+        self.end_point = end_point
+        self.voxel_model = np.zeros((3, 3, 3), dtype=self.dtype)
+        self.params = params
         self.keys = list(self.params.keys())
         self._make_model_params()
         self.voxel_space = self.params["voxel_space"]
@@ -302,26 +307,21 @@ class TuringModel_Cylinder(TuringModel_Rectangular):
 
     _names = ["_space", "_trabecular", "_cortical", "_subcutaneus", "_dermis", "_air"]
 
+    _PARAMS = {
+        "r_bone": 9.14, "voxel_space": 0.0245, "dicom_path": False, "bv_tv": 0.138,
+        "th_cortical": 1., "th_subcutaneus": 2.6, "th_dermis": 1.4,
+        "n_space": 1., "n_trabecular": 1.4, "n_cortical": 1.4, "n_subcutaneus": 1.4,
+        "n_dermis": 1.4, "n_air": 1.,
+        "ma_space": 1e-8, "ma_trabecular": 0.02374, "ma_cortical": 0.02374,
+        "ma_subcutaneus": 0.011, "ma_dermis": 0.037, "ma_air": 1e-5,
+        "ms_space": 1e-8, "ms_trabecular": 20.54, "ms_cortical": 17.67,
+        "ms_subcutaneus": 20, "ms_dermis": 20, "ms_air": 1e-5,
+        "g_space": 0.90, "g_trabecular": 0.90, "g_cortical": 0.90, "g_subcutaneus": 0.90,
+        "g_dermis": .90, "g_air": .90,
+    }
+
     def __init__(self):
-        super().__init__()
-        self.model_name = "TuringModel_Cylinder"
-        self.air_num = 5
-        self.end_point = 6
-        self.params = {
-            "r_bone": 9.14, "voxel_space": 0.0245, "dicom_path": False, "bv_tv": 0.138,
-            "th_cortical": 1., "th_subcutaneus": 2.6, "th_dermis": 1.4,
-            "n_space": 1., "n_trabecular": 1.4, "n_cortical": 1.4, "n_subcutaneus": 1.4,
-            "n_dermis": 1.4, "n_air": 1.,
-            "ma_space": 1e-8, "ma_trabecular": 0.02374, "ma_cortical": 0.02374,
-            "ma_subcutaneus": 0.011, "ma_dermis": 0.037, "ma_air": 1e-5,
-            "ms_space": 1e-8, "ms_trabecular": 20.54, "ms_cortical": 17.67,
-            "ms_subcutaneus": 20, "ms_dermis": 20, "ms_air": 1e-5,
-            "g_space": 0.90, "g_trabecular": 0.90, "g_cortical": 0.90, "g_subcutaneus": 0.90,
-            "g_dermis": .90, "g_air": .90,
-        }
-        self.keys = list(self.params.keys())
-        self._make_model_params()
-        self.voxel_space = self.params["voxel_space"]
+        self._init_model("TuringModel_Cylinder", dict(self._PARAMS), end_point=6, air_num=5)
 
     @staticmethod
     def round_index(X, num_r):
@@ -365,12 +365,9 @@ class TuringModel_RnC(TuringModel_Cylinder):
     """Rectangle-and-cylinder bone (pymopt/voxel_gpu/_classes.py:755-821)."""
 
     def __init__(self):
-        super().__init__()
-        self.model_name = "TuringModel_RnC"
-        self.params = dict(self.params)
-        self.params = {"r_bone": 9.14, "xz_size": 17.15, **{k: v for k, v in self.params.items()
-                                                          if k != "r_bone"}}
-        self.keys = list(self.params.keys())
+        params = {"r_bone": 9.14, "xz_size": 17.15,
+                  **{k: v for k, v in self._PARAMS.items() if k != "r_bone"}}
+        self._init_model("TuringModel_RnC", params, end_point=6, air_num=5)
 
     def _make_voxel_model(self):
         self._check_dicom()

@@ -162,11 +162,103 @@ def run_c3_case(ref_root: str, nph: int = 2000, seeds: int = 10, nr: int = 100,
     return out
 
 
+TURING_PARAMS = {"voxel_space": 0.1, "th_cortical": 1.0, "th_subcutaneus": 1.2, "th_dermis": 0.8}
+
+
+def bone_volume(seed: int = 0, shape=(60, 40, 60)) -> np.ndarray:
+    """Seeded binary stand-in for a Turing-pattern bone volume."""
+    rng = np.random.default_rng(seed)
+    return (rng.random(shape) < 0.3).astype(np.int8)
+
+
+def run_volumes_case(ref_root: str) -> str:
+    """Volumes built by the reference's own model classes (PlateModel,
+    PlateExModel, TuringModel_*; pymopt/voxel/_classes.py:343-782, identical
+    to pymopt/voxel_gpu/_classes.py:387-821), saved as an npz."""
+    _stub_modules()
+    sys.path.insert(0, ref_root)
+    if not hasattr(np, "int"):
+        np.int = int  # the reference's Turing models use the removed alias
+    from pymopt.voxel import _classes as RC
+    # pymopt/voxel/_classes.py calls tqdm without importing it
+    RC.tqdm = getattr(RC, "tqdm", lambda it: it)
+    out = {}
+    with contextlib.redirect_stdout(io.StringIO()):
+        m = RC.PlateModel()
+        m.set_params(x_size=2.1, y_size=1.6, voxel_space=0.1, thickness=[0.3, 0.5, 0.2],
+                     n=[1.4, 1.37, 1.45], n_air=1.0, ma=[0.1, 0.2, 0.3], ms=[10, 20, 30],
+                     g=[0.9, 0.8, 0.7])
+        m.build()
+        out["plate"] = m.voxel_model
+        m = RC.PlateExModel()
+        m.set_params(x_size=2.0, y_size=1.5, voxel_space=0.1, thickness=[0.3, 1.0],
+                     n=[1.5, 1.4], n_air=1.0, ma=[1e-5, 0.02], ms=[1e-5, 1.0], g=[0.9, 0.9])
+        m.build()
+        out["plate_ex"] = m.voxel_model
+        u = bone_volume()
+        out["bone"] = u
+        for name, extra in (("TuringModel_Rectangular", {"xz_size": 6.0}),
+                            ("TuringModel_Cylinder", {"r_bone": 3.5}),
+                            ("TuringModel_RnC", {"xz_size": 6.0, "r_bone": 3.5})):
+            m = getattr(RC, name)()
+            m.set_params(**TURING_PARAMS, **extra)
+            m.build(u.copy())
+            out[name] = m.voxel_model
+    path = os.path.join(HERE, "ref_volumes.npz")
+    np.savez_compressed(path, **out)
+    return path
+
+
+def run_sources_case(ref_root: str) -> str:
+    """Initial photon state the reference builds on the host
+    (_generate_initial_coodinate, pymopt/voxel/_classes.py:102-203) for the
+    beam options that do not draw random numbers, and the specular fraction
+    of initial_refrect_by_angle."""
+    _stub_modules()
+    sys.path.insert(0, ref_root)
+    from pymopt.voxel import _classes as RC
+    cases = []
+    base = dict(x_size=2.1, y_size=2.1, voxel_space=0.1, thickness=[0.5, 1.0],
+                n=[1.4, 1.5], n_air=1.0, ma=[0.1, 0.2], ms=[10, 20], g=[0.9, 0.8])
+    with contextlib.redirect_stdout(io.StringIO()):
+        for name, cls, kw in (
+                ("default", RC.VoxelPlateModel, {}),
+                ("angle", RC.VoxelPlateModel, {"beam_angle": 0.3}),
+                ("angle_refrect", RC.VoxelPlateModel,
+                 {"beam_angle": 0.3, "initial_refrect_by_angle": True}),
+                ("first_layer_clear", RC.VoxelPlateModel, {"first_layer_clear": True})):
+            m = cls(nPh=20000, **kw)
+            m.build(**base)
+            if name == "first_layer_clear":
+                m.model.get_second_layer_addz = lambda: 6
+            np.random.seed(0)
+            m._reset_results()
+            m._generate_initial_coodinate(m.nPh)
+            rec = {"name": name, "kwargs": kw, "params": base,
+                   "add": m.add[:, -1].tolist(), "p": m.p[:, -1].astype(float).tolist(),
+                   "v": m.v[:, -1].astype(float).tolist(), "w": float(m.w[-1]),
+                   "n_transported": int(m.w.size)}
+            if name == "angle_refrect":
+                rec["spec_fraction"] = float(m.inital_del_num / m.nPh)
+                rec["spec_v"] = m.v_result[:, -1].astype(float).tolist()
+            cases.append(rec)
+    path = os.path.join(HERE, "ref_sources.json")
+    with open(path, "w") as f:
+        json.dump({"generator": "tests/golden/make_golden.py", "cases": cases}, f, indent=1)
+    return path
+
+
 def main():
     ref_root = sys.argv[1]
-    cases = sys.argv[2:] or list(PLATE_CASES) + ["c3"]
+    cases = sys.argv[2:] or list(PLATE_CASES) + ["c3", "volumes", "sources"]
     for name in cases:
         t0 = time.time()
+        if name == "volumes":
+            print("volumes ->", run_volumes_case(ref_root))
+            continue
+        if name == "sources":
+            print("sources ->", run_sources_case(ref_root))
+            continue
         res = run_c3_case(ref_root) if name == "c3" else run_plate_case(ref_root, name)
         res["generator"] = "tests/golden/make_golden.py (reference pymopt.voxel, Numba)"
         path = os.path.join(HERE, f"ref_{name}.json")
