@@ -200,6 +200,24 @@ int pmo_run_plain(const pmo_problem *prob, const pmo_tallies *tal,
                   size_t workspace_bytes, void *stream);
 
 /*
+ * pmo_run_plain without a caller-allocated workspace.  No counterpart in the
+ * reference.  For callers that cannot allocate device memory themselves (a
+ * plugin in a host application that owns all device memory through its own
+ * pool, or a path where cudaMalloc, which may synchronise the device, is not
+ * allowed): the scratch lives in a file-scope device array of
+ * PMO_STATIC_WORKSPACE_BYTES bytes that every GPU loading the library holds
+ * until exit.  Returns PMO_ERR_WORKSPACE if the run needs more scratch than
+ * that.  The first call on a device looks up the array's device address with
+ * that device current; make that first call before any stream capture.  All
+ * calls share the array: calls on one stream in sequence are fine, calls that
+ * overlap on the GPU (other streams or host threads) race on it.  Allocates
+ * nothing; the caller still passes the problem and the tally buffers.
+ */
+#define PMO_STATIC_WORKSPACE_BYTES 512
+int pmo_run_plain_static(const pmo_problem *prob, const pmo_tallies *tal,
+                         const pmo_launch *launch, void *stream);
+
+/*
  * Drop-in for the reference kernel cuVMC (pymopt/voxel_gpu/_cukernel.py:27-35):
  * same argument list and meaning (SoA state add[3*nPh], p[3*nPh], v[3*nPh],
  * w[nPh] updated in place; ma/ms/g indexed by label < end_point; n indexed

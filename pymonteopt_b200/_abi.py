@@ -71,6 +71,7 @@ PMO_FLAG_EXPORT_EXITS = 1
 PMO_FLAG_PHOTON_STATS = 2
 
 PMO_WS_LEDGER_OFFSET = 64
+PMO_STATIC_WORKSPACE_BYTES = 512
 PMO_WS_COUNTERS_OFFSET = 256
 
 STATUS_NAMES = {
