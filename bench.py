@@ -142,11 +142,12 @@ def cpu_oracle_rate(target_seconds: float, seed: int = 1234) -> dict:
     from pymonteopt_b200 import volumes as V
     prob = V.c2_skin()
     threads = host_threads()
-    n = max(200, 50 * threads)
+    oracle.load()                      # build/load outside the timed calibration
+    n = max(2000, 200 * threads)
     t0 = time.perf_counter()
     oracle.run(prob, n, seed, precision=A.PMO_FP32, nr=100, dr=0.1, threads=threads)
     dt = time.perf_counter() - t0
-    n2 = int(max(n, min(5e7, n * target_seconds / max(dt, 1e-3))))
+    n2 = int(max(n, min(5e8, n * target_seconds / max(dt, 1e-3))))
     t0 = time.perf_counter()
     r = oracle.run(prob, n2, seed + 1, begin=n, precision=A.PMO_FP32, nr=100, dr=0.1,
                    threads=threads)
