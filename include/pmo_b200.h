@@ -103,6 +103,8 @@ extern "C" {
 /* ---- run flags ---------------------------------------------------------- */
 #define PMO_FLAG_EXPORT_EXITS  1u  /* write per-photon final state arrays        */
 #define PMO_FLAG_PHOTON_STATS  2u  /* write per-photon event counts (validation) */
+#define PMO_FLAG_SCORE_RECORD  4u  /* write per-photon exit bin and weight, the
+                                      input of the gradient replay             */
 
 typedef struct pmo_problem {
     /* geometry: padded label volume, C-order (nx, ny, nz) */
@@ -164,7 +166,51 @@ typedef struct pmo_tallies {
     float *exit_p, *exit_v, *exit_w;
     /* PMO_FLAG_PHOTON_STATS: per-photon interaction / crossing / Fresnel counts */
     uint32_t *ph_interact, *ph_cross, *ph_fresnel;
+    /* PMO_FLAG_SCORE_RECORD: per photon, the R(r)/T(r) bin its exit weight went
+       to (category * nr + bin, -1 for none) and that weight */
+    int32_t *score_bin;
+    float *score_w;
 } pmo_tallies;
+
+/*
+ * Gradient replay (pmo_run_grad).  The forward run wrote score records; the
+ * loss gradient with respect to the binned exit weight is `coef`
+ * ([PMO_RR_CATS][nr]: dLoss / d(sum of exit weights in bin)).  Each photon
+ * with q = coef[bin] * w != 0 is replayed from its Philox counters and
+ * contributes the perturbation Monte Carlo terms of implicit-capture
+ * weighting: for every voxel v it crossed, dLoss/dmu_a(v) += -q * L_v and
+ * dLoss/dmu_s(v) += q * (n_v / mu_s(v) - L_v), with L_v its path length and n_v
+ * its interactions in v.  Outputs are accumulated, never cleared.
+ */
+typedef struct pmo_grad {
+    const float *coef;               /* PMO_RR_CATS * nr */
+    int32_t nr;
+    float dr;
+    const int32_t *score_bin;        /* forward records, index photon - begin */
+    const float *score_w;
+    float *d_ma_voxel, *d_ms_voxel;  /* nx*ny*nz or NULL (needs voxel stepping) */
+    double *d_ma_label, *d_ms_label; /* n_labels or NULL */
+    unsigned long long *counters;    /* PMO_G_* */
+    /* optional central finite difference by reweighting the same photons
+       (perturbation Monte Carlo), for up to PMO_FD_MAX targets: fd_target maps
+       every voxel to a target index or -1; target t scales mu_a (fd_param 0)
+       or mu_s (fd_param 1) of its voxels by (1 +- fd_h).  fd_out[2 * t + 0/1]
+       accumulates sum over replayed photons of coef[bin] * w * (f -+ 1), with
+       f = (1 +- h)^n_t * exp(-(+-h) mu_t_param L_t) (mu_s) or exp(-(+-h) mu_a L_t)
+       (mu_a); (fd_out[2t] - fd_out[2t+1]) / (2 h mu) is the central difference. */
+    const int16_t *fd_target;        /* nx*ny*nz or NULL */
+    int32_t fd_n;
+    int32_t fd_param;
+    float fd_h;
+    double *fd_out;                  /* 2 * fd_n */
+} pmo_grad;
+
+#define PMO_FD_MAX 32
+
+#define PMO_G_REPLAYED   0           /* photons replayed (q != 0)               */
+#define PMO_G_SKIPPED    1           /* photons with q == 0                     */
+#define PMO_G_MISMATCH   2           /* replay ended in another bin or weight   */
+#define PMO_G_COUNTERS_N 4
 
 typedef struct pmo_launch {
     int32_t block_threads;       /* 0 = default */
@@ -198,6 +244,17 @@ size_t pmo_workspace_bytes(void);
 int pmo_run_plain(const pmo_problem *prob, const pmo_tallies *tal,
                   const pmo_launch *launch, void *workspace,
                   size_t workspace_bytes, void *stream);
+
+/*
+ * Backward kernel: replay the photons of a forward run (same problem, seed
+ * and photon range; the forward ran with PMO_FLAG_SCORE_RECORD) and
+ * accumulate dLoss/dmu_a and dLoss/dmu_s per voxel and per label.  With
+ * per-voxel outputs the problem must step voxel by voxel (voxel_words NULL),
+ * in the forward run as well.  No counterpart in the reference, which has no
+ * derivatives.
+ */
+int pmo_run_grad(const pmo_problem *prob, const pmo_grad *grad, const pmo_launch *launch,
+                 void *workspace, size_t workspace_bytes, void *stream);
 
 /*
  * pmo_run_plain without a caller-allocated workspace.  No counterpart in the

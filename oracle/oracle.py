@@ -37,6 +37,9 @@ class OracleTallies(C.Structure):
         ("absorbed", C.c_void_p),
         ("ph_state", C.c_void_p),
         ("ph_counts", C.c_void_p),
+        ("grad_coef", C.c_void_p),
+        ("g_ma_voxel", C.c_void_p), ("g_ms_voxel", C.c_void_p),
+        ("g_ma_label", C.c_void_p), ("g_ms_label", C.c_void_p),
     ]
 
 
@@ -76,8 +79,13 @@ def _ptr(a):
 
 def run(prob, n_photons: int, seed: int, *, begin: int = 0, precision: int = A.PMO_FP64,
         nr: int = 0, dr: float = 0.1, fluence: bool = False, per_photon: bool = False,
-        threads: int = 0, max_events: int = 0, validate: bool = True) -> dict:
-    """Trace photons ``[begin, begin + n_photons)`` of ``prob`` on the CPU."""
+        threads: int = 0, max_events: int = 0, validate: bool = True,
+        grad_coef=None) -> dict:
+    """Trace photons ``[begin, begin + n_photons)`` of ``prob`` on the CPU.
+
+    ``grad_coef`` ([PMO_RR_CATS, nr] dLoss/d(bin weight sum)) also returns the
+    perturbation Monte Carlo derivatives per voxel and per label
+    (``g_ma_voxel``, ``g_ms_voxel``, ``g_ma_label``, ``g_ms_label``)."""
     lib = load()
     if validate:
         prob.validate()
@@ -110,6 +118,17 @@ def run(prob, n_photons: int, seed: int, *, begin: int = 0, precision: int = A.P
     t.rr, t.nr, t.dr = _ptr(rr), int(nr), float(dr)
     t.absorbed = _ptr(absorbed)
     t.ph_state, t.ph_counts = _ptr(ph_state), _ptr(ph_counts)
+    grads = {}
+    if grad_coef is not None:
+        if nr <= 0:
+            raise ValueError("gradients need R(r) bins (nr > 0)")
+        gc = np.ascontiguousarray(np.asarray(grad_coef, np.float64).reshape(A.PMO_RR_CATS, nr))
+        keep.append(gc)
+        grads = {"g_ma_voxel": np.zeros(prob.labels.shape), "g_ms_voxel": np.zeros(prob.labels.shape),
+                 "g_ma_label": np.zeros(prob.n_labels), "g_ms_label": np.zeros(prob.n_labels)}
+        t.grad_coef = gc.ctypes.data
+        for k, v in grads.items():
+            setattr(t, k, v.ctypes.data)
     if threads <= 0:
         threads = os.cpu_count() or 1
     status = lib.oracle_run(C.byref(s), C.byref(t), int(threads))
@@ -123,4 +142,5 @@ def run(prob, n_photons: int, seed: int, *, begin: int = 0, precision: int = A.P
         "ph_state": ph_state,
         "ph_counts": ph_counts,
         "threads": threads,
+        **grads,
     }

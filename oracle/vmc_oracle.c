@@ -37,12 +37,59 @@ typedef struct oracle_tallies {
     double *absorbed;     /* nx*ny*nz or NULL */
     double *ph_state;     /* 10 per photon: p[3], v[3], w, add[3]; or NULL */
     uint32_t *ph_counts;  /* 4 per photon: interactions, crossings, fresnel, status */
+    /* perturbation Monte Carlo gradient (all NULL or all set): for a photon
+       whose exit weight w lands in bin b, q = grad_coef[b] * w is spread over
+       the voxels it crossed: g_ma += -q*L, g_ms += q*(n/mu_s - L) */
+    const double *grad_coef;          /* PMO_RR_CATS * nr */
+    double *g_ma_voxel, *g_ms_voxel;  /* nx*ny*nz */
+    double *g_ma_label, *g_ms_label;  /* n_labels */
 } oracle_tallies;
 
+/* per-thread scratch: ledger, counters and a photon's cell log */
 typedef struct {
     double ledger[PMO_LEDGER_N];
     unsigned long long counters[PMO_COUNTERS_N];
+    int nseg, capseg;
+    int64_t *seg_lin;
+    int *seg_lab;
+    double *seg_L, *seg_N;
 } oracle_acc;
+
+static void seg_push(oracle_acc *acc, int64_t lin, int lab, double L, double N) {
+    if (L == 0.0 && N == 0.0) return;
+    if (acc->nseg == acc->capseg) {
+        int cap = acc->capseg ? 2 * acc->capseg : 256;
+        acc->seg_lin = (int64_t *)realloc(acc->seg_lin, cap * sizeof(int64_t));
+        acc->seg_lab = (int *)realloc(acc->seg_lab, cap * sizeof(int));
+        acc->seg_L = (double *)realloc(acc->seg_L, cap * sizeof(double));
+        acc->seg_N = (double *)realloc(acc->seg_N, cap * sizeof(double));
+        acc->capseg = cap;
+    }
+    acc->seg_lin[acc->nseg] = lin;
+    acc->seg_lab[acc->nseg] = lab;
+    acc->seg_L[acc->nseg] = L;
+    acc->seg_N[acc->nseg] = N;
+    acc->nseg++;
+}
+
+static void seg_apply(oracle_acc *acc, const oracle_tallies *tal, double q) {
+    for (int i = 0; i < acc->nseg; ++i) {
+        const double dma = -q * acc->seg_L[i];
+        const double dms = q * acc->seg_N[i] - q * acc->seg_L[i];
+        if (tal->g_ma_voxel) {
+#pragma omp atomic
+            tal->g_ma_voxel[acc->seg_lin[i]] += dma;
+#pragma omp atomic
+            tal->g_ms_voxel[acc->seg_lin[i]] += dms;
+        }
+        if (tal->g_ma_label) {
+#pragma omp atomic
+            tal->g_ma_label[acc->seg_lab[i]] += dma;
+#pragma omp atomic
+            tal->g_ms_label[acc->seg_lab[i]] += dms;
+        }
+    }
+}
 
 /* ---- FP32 build ---- */
 #define REAL float

@@ -12,7 +12,7 @@
 #define PFX(name) PMO_CAT(name, SUFFIX)
 
 typedef struct {
-    REAL mt, imt, ma_mt, ma, ms, n, g;
+    REAL mt, imt, ma_mt, ma, ms, n, g, ims;
     REAL hgA, hgB, hgC, hgD, hgE;
     int valid;
 } PFX(props_t);
@@ -30,6 +30,7 @@ static void PFX(make_props)(PFX(props_t) *t, float ma, float ms, float g, float 
     t->hgC = 1 - gg;
     t->hgD = 2 * gg;
     t->hgE = gg != 0 ? (REAL)1 / (2 * gg) : (REAL)0;
+    t->ims = ms > 0 ? (REAL)1 / (REAL)ms : (REAL)0;
     t->valid = valid;
 }
 
@@ -67,6 +68,10 @@ static int PFX(trace)(const pmo_problem *P, const PFX(props_t) *tab,
     REAL p[3], v[3], w;
     int status = PMO_OK;
     uint32_t n_int = 0, n_cross = 0, n_fres = 0, events = 0;
+    /* gradient: path length and sum of 1/mu_s in the current voxel */
+    const int grad = tal->grad_coef != NULL;
+    double gL = 0.0, gN = 0.0;
+    acc->nseg = 0;
 
     /* ---- source (pymopt/voxel_gpu/_classes.py:148-254) ---- */
     ctr[0] = 0; ctr[1] = 2; ctr[2] = idlo; ctr[3] = idhi;
@@ -147,10 +152,12 @@ static int PFX(trace)(const pmo_problem *P, const PFX(props_t) *tab,
                 /* hop inside the voxel (:170-175) */
                 REAL s = st * cur.imt;
                 for (int a = 0; a < 3; ++a) p[a] += v[a] * s;
+                gL += (double)s;
                 break;
             }
             /* move to the face and snap (:92-96) */
             for (int a = 0; a < 3; ++a) p[a] += v[a] * db;
+            gL += (double)db;
             p[ax] = PFX(sgn)(v[ax]) * hl;
             st -= dbmt;
             n_cross++;
@@ -211,6 +218,7 @@ static int PFX(trace)(const pmo_problem *P, const PFX(props_t) *tab,
             if (!transmit) continue;
             /* cross into the neighbour (:137-148, :156-167) */
             if (nlab == lab && P->props_mode == PMO_PROPS_LABEL) acc->counters[PMO_C_SAMECROSS]++;
+            if (grad) { seg_push(acc, lin, lab, gL, gN); gL = gN = 0.0; }
             c[ax] = nc;
             lin = nlin;
             p[ax] = -p[ax];
@@ -241,6 +249,7 @@ static int PFX(trace)(const pmo_problem *P, const PFX(props_t) *tab,
                             int b = (int)q - 1;
 #pragma omp atomic
                             tal->rr[cat * tal->nr + b] += wd;
+                            if (grad) seg_apply(acc, tal, tal->grad_coef[cat * tal->nr + b] * wd);
                         }
                     }
                 }
@@ -254,6 +263,7 @@ static int PFX(trace)(const pmo_problem *P, const PFX(props_t) *tab,
                 cur = tab[lab];
         }
 
+        gN += (double)cur.ims;
         /* absorption, implicit capture (:179) */
         {
             REAL wn = w - w * cur.ma_mt;
@@ -344,6 +354,7 @@ int PFX(oracle_run)(const pmo_problem *P, oracle_tallies *tal, int threads) {
     {
         oracle_acc acc;
         memset(&acc, 0, sizeof(acc));
+        (void)seg_push;
         int st_local = PMO_OK;
 #pragma omp for schedule(dynamic, 64)
         for (int64_t k = 0; k < (int64_t)P->photon_count; ++k) {
@@ -356,6 +367,10 @@ int PFX(oracle_run)(const pmo_problem *P, oracle_tallies *tal, int threads) {
             for (int i = 0; i < PMO_COUNTERS_N; ++i) tal->counters[i] += acc.counters[i];
             if (st_local != PMO_OK) worst = st_local;
         }
+        free(acc.seg_lin);
+        free(acc.seg_lab);
+        free(acc.seg_L);
+        free(acc.seg_N);
     }
     return worst;
 }

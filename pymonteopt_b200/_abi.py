@@ -69,6 +69,13 @@ PMO_RR_CATS = 4
 
 PMO_FLAG_EXPORT_EXITS = 1
 PMO_FLAG_PHOTON_STATS = 2
+PMO_FLAG_SCORE_RECORD = 4
+
+PMO_G_REPLAYED = 0
+PMO_G_SKIPPED = 1
+PMO_G_MISMATCH = 2
+PMO_G_COUNTERS_N = 4
+PMO_FD_MAX = 32
 
 PMO_WS_LEDGER_OFFSET = 64
 PMO_STATIC_WORKSPACE_BYTES = 512
@@ -134,6 +141,24 @@ class PmoTallies(C.Structure):
         ("exit_add", C.c_void_p), ("exit_p", C.c_void_p),
         ("exit_v", C.c_void_p), ("exit_w", C.c_void_p),
         ("ph_interact", C.c_void_p), ("ph_cross", C.c_void_p), ("ph_fresnel", C.c_void_p),
+        ("score_bin", C.c_void_p), ("score_w", C.c_void_p),
+    ]
+
+
+class PmoGrad(C.Structure):
+    _fields_ = [
+        ("coef", C.c_void_p),
+        ("nr", C.c_int32),
+        ("dr", C.c_float),
+        ("score_bin", C.c_void_p), ("score_w", C.c_void_p),
+        ("d_ma_voxel", C.c_void_p), ("d_ms_voxel", C.c_void_p),
+        ("d_ma_label", C.c_void_p), ("d_ms_label", C.c_void_p),
+        ("counters", C.c_void_p),
+        ("fd_target", C.c_void_p),
+        ("fd_n", C.c_int32),
+        ("fd_param", C.c_int32),
+        ("fd_h", C.c_float),
+        ("fd_out", C.c_void_p),
     ]
 
 

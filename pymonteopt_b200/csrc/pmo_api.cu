@@ -11,6 +11,8 @@ cudaError_t launch_plain_f32(const KParams &kp, int props, int flu, int threads,
                              cudaStream_t s, LaunchShape *out);
 cudaError_t launch_plain_f64(const KParams &kp, int props, int flu, int threads, int bps,
                              cudaStream_t s, LaunchShape *out);
+cudaError_t launch_grad_f32(const KParams &kp, int props, int threads, int bps, cudaStream_t s);
+cudaError_t launch_grad_f64(const KParams &kp, int props, int threads, int bps, cudaStream_t s);
 
 // phi = absorbed / (n_photons * l^3 * mu_a) over the interior voxels, FP64.
 __global__ void normalize_fluence_kernel(const float *__restrict__ absorbed,
@@ -173,6 +175,10 @@ int tallies_to_params(const pmo_problem *p, const pmo_tallies *t, KParams *kp) {
     kp->ph_interact = t->ph_interact;
     kp->ph_cross = t->ph_cross;
     kp->ph_fresnel = t->ph_fresnel;
+    if ((p->flags & PMO_FLAG_SCORE_RECORD) && (!t->score_bin || !t->score_w || t->nr <= 0))
+        return PMO_ERR_ARG;
+    kp->score_bin = t->score_bin;
+    kp->score_w = t->score_w;
     return PMO_OK;
 }
 
@@ -235,6 +241,57 @@ int pmo_run_plain(const pmo_problem *prob, const pmo_tallies *tal, const pmo_lau
     if (prob->photon_count == 0) return PMO_OK;
     return launch_kp(kp, prob->precision, prob->props_mode, tal->fluence_mode, launch,
                      static_cast<cudaStream_t>(stream));
+}
+
+int pmo_run_grad(const pmo_problem *prob, const pmo_grad *g, const pmo_launch *launch,
+                 void *workspace, size_t workspace_bytes, void *stream) {
+    KParams kp;
+    int st = problem_to_params(prob, &kp);
+    if (st != PMO_OK) return st;
+    if (!g || !g->coef || g->nr <= 0 || !finite_pos(g->dr) || !g->score_bin || !g->score_w ||
+        !g->counters)
+        return PMO_ERR_ARG;
+    if ((g->d_ma_voxel == nullptr) != (g->d_ms_voxel == nullptr)) return PMO_ERR_ARG;
+    if ((g->d_ma_label == nullptr) != (g->d_ms_label == nullptr)) return PMO_ERR_ARG;
+    if (!g->d_ma_voxel && !g->d_ma_label) return PMO_ERR_ARG;
+    // per-voxel derivatives need the voxel-by-voxel path
+    if (g->d_ma_voxel && prob->voxel_words) return PMO_ERR_ARG;
+    if (!workspace || workspace_bytes < kWorkspaceBytes) return PMO_ERR_WORKSPACE;
+    if (prob->photon_count == 0) return PMO_OK;
+    int threads = launch && launch->block_threads > 0 ? launch->block_threads : 128;
+    if (threads % 32 != 0 || threads > 512) return PMO_ERR_ARG;
+    unsigned char *ws = static_cast<unsigned char *>(workspace);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (cudaMemsetAsync(ws, 0, kWorkspaceBytes, s) != cudaSuccess) return PMO_ERR_CUDA;
+    kp.work = reinterpret_cast<unsigned long long *>(ws);
+    kp.ledger = reinterpret_cast<double *>(ws + kWsLedgerOff);
+    kp.counters = reinterpret_cast<unsigned long long *>(ws + kWsCountersOff);
+    kp.nr = g->nr;
+    kp.dr = g->dr;
+    kp.coef = g->coef;
+    kp.score_bin = const_cast<int32_t *>(g->score_bin);
+    kp.score_w = const_cast<float *>(g->score_w);
+    kp.d_ma_voxel = g->d_ma_voxel;
+    kp.d_ms_voxel = g->d_ms_voxel;
+    kp.d_ma_label = g->d_ma_label;
+    kp.d_ms_label = g->d_ms_label;
+    kp.gcounters = g->counters;
+    if (g->fd_n > 0) {
+        if (g->fd_n > PMO_FD_MAX || !g->fd_target || !g->fd_out || !(g->fd_h > 0.f) ||
+            (g->fd_param != 0 && g->fd_param != 1))
+            return PMO_ERR_ARG;
+        kp.fd_target = g->fd_target;
+        kp.fd_n = g->fd_n;
+        kp.fd_param = g->fd_param;
+        kp.fd_h = g->fd_h;
+        kp.fd_out = g->fd_out;
+    }
+    kp.flags = 0;
+    const int bps = launch ? launch->blocks_per_sm : 0;
+    cudaError_t e = prob->precision == PMO_FP64
+                        ? pmo::launch_grad_f64(kp, prob->props_mode, threads, bps, s)
+                        : pmo::launch_grad_f32(kp, prob->props_mode, threads, bps, s);
+    return e == cudaSuccess ? PMO_OK : PMO_ERR_CUDA;
 }
 
 int pmo_cuvmc(int32_t *add, float *p, float *v, float *w, const float *ma, const float *ms,

@@ -47,6 +47,17 @@ struct KParams {
     int32_t *exit_add;
     float *exit_p, *exit_v, *exit_w;
     uint32_t *ph_interact, *ph_cross, *ph_fresnel;
+    int32_t *score_bin;            // forward: written; gradient replay: read
+    float *score_w;
+    // gradient replay
+    const float *coef;             // dLoss/d(bin weight), [PMO_RR_CATS][nr]
+    float *d_ma_voxel, *d_ms_voxel;
+    double *d_ma_label, *d_ms_label;
+    unsigned long long *gcounters;
+    const int16_t *fd_target;      // pMC-reweighted central difference
+    int32_t fd_n, fd_param;
+    float fd_h;
+    double *fd_out;
     // scratch: [0] next photon chunk
     unsigned long long *work;
 };
@@ -59,6 +70,8 @@ struct LaunchShape {
 };
 
 // vmc_plain.cu
+cudaError_t launch_grad(const KParams &kp, int precision, int props_mode, int block_threads,
+                        int blocks_per_sm, cudaStream_t stream);
 cudaError_t launch_plain(const KParams &kp, int precision, int props_mode, int fluence_mode,
                          int block_threads, int blocks_per_sm, cudaStream_t stream,
                          LaunchShape *shape_out);

@@ -20,11 +20,12 @@ inline int device_sm_count() {
     return cached[dev];
 }
 
-template <typename R, int PROPS, int FLU, bool SKIP>
+template <typename R, int PROPS, int FLU, bool SKIP, bool GRAD = false>
 cudaError_t launch_plain_t(const KParams &kp, int threads, int blocks_per_sm, cudaStream_t s,
                            LaunchShape *out) {
-    auto kern = vmc_plain_kernel<R, PROPS, FLU, SKIP>;
-    const size_t smem = SmemLayout<R>::total(kp.nr, kp.rr_shared, FLU, kp.win_dim);
+    auto kern = vmc_plain_kernel<R, PROPS, FLU, SKIP, GRAD>;
+    size_t smem = SmemLayout<R>::total(kp.nr, kp.rr_shared, FLU, kp.win_dim);
+    if (GRAD && kp.fd_n > 0) smem += SmemLayout<R>::fd_bytes(threads);
     cudaError_t e;
     if (smem > 48 * 1024) {
         e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -73,6 +74,21 @@ cudaError_t launch_plain_r(const KParams &kp, int props, int flu, int threads, i
     if (flu == PMO_FLU_GLOBAL)
         return launch_plain_t<R, PMO_PROPS_VOXEL, PMO_FLU_GLOBAL, false>(kp, threads, bps, s, out);
     return launch_plain_t<R, PMO_PROPS_VOXEL, PMO_FLU_SHARED, false>(kp, threads, bps, s, out);
+}
+
+// Gradient replay: no fluence; uniform boxes only when the problem carries a
+// voxel-word map (per-label derivatives only).
+template <typename R>
+cudaError_t launch_grad_r(const KParams &kp, int props, int threads, int bps, cudaStream_t s) {
+    if (props == PMO_PROPS_LABEL) {
+        if (kp.words)
+            return launch_plain_t<R, PMO_PROPS_LABEL, PMO_FLU_NONE, true, true>(kp, threads, bps, s,
+                                                                                nullptr);
+        return launch_plain_t<R, PMO_PROPS_LABEL, PMO_FLU_NONE, false, true>(kp, threads, bps, s,
+                                                                             nullptr);
+    }
+    return launch_plain_t<R, PMO_PROPS_VOXEL, PMO_FLU_NONE, false, true>(kp, threads, bps, s,
+                                                                         nullptr);
 }
 
 }  // namespace pmo

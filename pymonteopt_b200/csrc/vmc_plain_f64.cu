@@ -9,4 +9,8 @@ cudaError_t launch_plain_f64(const KParams &kp, int props, int flu, int threads,
                              cudaStream_t s, LaunchShape *out) {
     return launch_plain_r<double>(kp, props, flu, threads, bps, s, out);
 }
+cudaError_t launch_grad_f64(const KParams &kp, int props, int threads, int bps,
+                            cudaStream_t s) {
+    return launch_grad_r<double>(kp, props, threads, bps, s);
+}
 }  // namespace pmo

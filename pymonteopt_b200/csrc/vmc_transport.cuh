@@ -27,14 +27,29 @@ template <typename R>
 struct __align__(16) LabelProps {
     R mt, imt, ma_mt, n;       // mu_t, 1/mu_t, mu_a/mu_t, refractive index
     R hgA, hgB, hgC, hgE;      // 1+g^2, 1-g^2, 1-g, 1/(2g) (0 when g == 0)
-    R hgD, pad0, pad1, pad2;   // 2g
+    R hgD, ims, pad1, pad2;    // 2g, 1/mu_s (0 when mu_s == 0)
 };
 
-// ---- arithmetic helpers: fast single-precision forms for the product,
-// IEEE double forms for the FP64 build (its translation unit also disables
-// FMA contraction so that it rounds like the CPU oracle).
-__device__ __forceinline__ float plog(float x) { return __logf(x); }
-__device__ __forceinline__ double plog(double x) { return log(x); }
+// ---- arithmetic.  Every single-precision add, multiply, fused multiply-add
+// and divide on the photon path is an explicitly rounded intrinsic, so the
+// compiler cannot fuse or split them differently in different kernel
+// instantiations: the gradient replay then follows the forward run's photon
+// paths bit for bit.  The FP64 build uses plain operators in a translation
+// unit compiled with -fmad=false, which round every operation separately in
+// the order the CPU oracle does.
+__device__ __forceinline__ float xmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float xadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float xsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float xfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ float xdiv(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ double xmul(double a, double b) { return a * b; }
+__device__ __forceinline__ double xadd(double a, double b) { return a + b; }
+__device__ __forceinline__ double xsub(double a, double b) { return a - b; }
+__device__ __forceinline__ double xfma(double a, double b, double c) { return a * b + c; }
+__device__ __forceinline__ double xdiv(double a, double b) { return a / b; }
+// -ln(u) for u in (0, 1]
+__device__ __forceinline__ float pneglog(float u) { return __fmul_rn(__log2f(u), -0.69314718055994531f); }
+__device__ __forceinline__ double pneglog(double u) { return -log(u); }
 __device__ __forceinline__ float psqrt(float x) { return sqrtf(x); }
 __device__ __forceinline__ double psqrt(double x) { return sqrt(x); }
 __device__ __forceinline__ float pinvnorm(float s) { return rsqrtf(s); }
@@ -43,7 +58,7 @@ __device__ __forceinline__ double pinvnorm(double s) { return 1.0 / sqrt(s); }
 __device__ __forceinline__ void psincos2pi(float u, float *s, float *c) {
     // 2*pi*(u - 1/2) lies in (-pi, pi], where the hardware sine is accurate;
     // sin(x + pi) = -sin(x), cos(x + pi) = -cos(x).
-    float a = 6.28318530717958647692f * (u - 0.5f);
+    const float a = __fmul_rn(6.28318530717958647692f, __fsub_rn(u, 0.5f));
     float ss, cc;
     __sincosf(a, &ss, &cc);
     *s = -ss;
@@ -54,32 +69,38 @@ __device__ __forceinline__ void psincos2pi(double u, double *s, double *c) {
 }
 template <typename R>
 __device__ __forceinline__ R sgn(R x) { return signbit(x) ? R(-1) : R(1); }
+// sum of squares in the oracle's order ((x*x + y*y) + z*z)
+template <typename R>
+__device__ __forceinline__ R sumsq(R x, R y, R z) {
+    return xfma(z, z, xfma(y, y, xmul(x, x)));
+}
 
 template <typename R>
 __device__ __forceinline__ void make_props(LabelProps<R> &t, float ma, float ms, float g,
                                            float n) {
-    t.mt = (R)ma + (R)ms;
-    t.imt = t.mt > R(0) ? R(1) / t.mt : R(0);
-    t.ma_mt = t.mt > R(0) ? (R)ma / t.mt : R(0);
+    t.mt = xadd((R)ma, (R)ms);
+    t.imt = t.mt > R(0) ? xdiv(R(1), t.mt) : R(0);
+    t.ma_mt = t.mt > R(0) ? xdiv((R)ma, t.mt) : R(0);
     t.n = (R)n;
-    R gg = (R)g;
-    t.hgA = 1 + gg * gg;
-    t.hgB = 1 - gg * gg;
-    t.hgC = 1 - gg;
-    t.hgD = 2 * gg;
-    t.hgE = gg != R(0) ? R(1) / (2 * gg) : R(0);
-    t.pad0 = t.pad1 = t.pad2 = R(0);
+    const R gg = (R)g;
+    t.hgA = xfma(gg, gg, R(1));
+    t.hgB = xfma(-gg, gg, R(1));
+    t.hgC = xsub(R(1), gg);
+    t.hgD = xmul(R(2), gg);
+    t.hgE = gg != R(0) ? xdiv(R(1), xmul(R(2), gg)) : R(0);
+    t.ims = ms > 0.f ? xdiv(R(1), (R)ms) : R(0);
+    t.pad1 = t.pad2 = R(0);
 }
 
 // theta(g, rand) of the reference (pymopt/voxel_gpu/_cukernel.py:14-25)
 template <typename R>
 __device__ __forceinline__ R hg_cos(const LabelProps<R> &t, R u) {
     if (t.hgE != R(0)) {
-        R q = t.hgB / (t.hgC + t.hgD * u);
-        R c = (t.hgA - q * q) * t.hgE;
+        const R q = xdiv(t.hgB, xfma(t.hgD, u, t.hgC));
+        const R c = xmul(xfma(-q, q, t.hgA), t.hgE);
         return c < R(-1) ? R(-1) : c;
     }
-    return 2 * u - 1;
+    return xsub(xmul(R(2), u), R(1));
 }
 
 // Dynamic shared memory layout of a transport block.
@@ -89,7 +110,8 @@ struct SmemLayout {
     static constexpr size_t led_off = tab_bytes;
     static constexpr size_t cnt_off = led_off + PMO_LEDGER_N * sizeof(double);
     static constexpr size_t valid_off = cnt_off + PMO_COUNTERS_N * sizeof(unsigned long long);
-    static constexpr size_t rr_off = valid_off + 256;
+    static constexpr size_t gl_off = valid_off + 256;  // per-label gradient sums
+    static constexpr size_t rr_off = gl_off + 2 * 256 * sizeof(double);
     __host__ __device__ static size_t win_off(int nr, int rr_shared) {
         size_t o = rr_off + (rr_shared ? (size_t)PMO_RR_CATS * nr * sizeof(R) : 0);
         return (o + 15) & ~size_t(15);
@@ -97,13 +119,23 @@ struct SmemLayout {
     __host__ __device__ static size_t total(int nr, int rr_shared, int flu, const int32_t win_dim[3]) {
         size_t o = win_off(nr, rr_shared);
         if (flu == PMO_FLU_SHARED) o += (size_t)win_dim[0] * win_dim[1] * win_dim[2] * sizeof(float);
-        return o;
+        return (o + 15) & ~size_t(15);
+    }
+    // gradient replay with the reweighted finite difference: per-target sums
+    // (2 * PMO_FD_MAX doubles) and per-thread target accumulators
+    __host__ __device__ static size_t fd_bytes(int threads) {
+        return 2 * PMO_FD_MAX * sizeof(double) + (size_t)threads * 2 * PMO_FD_MAX * sizeof(float);
     }
 };
 
 enum : int { kChunk = 64 };
 
-template <typename R, int PROPS, int FLU, bool SKIP>
+// GRAD: the gradient replay (pmo_run_grad).  It replays the photons whose
+// forward score record gives q = coef[bin] * w != 0 along the same path (same
+// arithmetic, same Philox draws) and accumulates -q*L and q*(n/mu_s - L) per
+// cell it crosses (a voxel, or a label-uniform box when only per-label
+// derivatives are asked for).
+template <typename R, int PROPS, int FLU, bool SKIP, bool GRAD = false>
 __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     using L = SmemLayout<R>;
@@ -112,8 +144,16 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
     unsigned long long *s_cnt = reinterpret_cast<unsigned long long *>(smem_raw + L::cnt_off);
     uint8_t *s_valid = smem_raw + L::valid_off;
     R *s_rr = reinterpret_cast<R *>(smem_raw + L::rr_off);
+    double *s_gma = reinterpret_cast<double *>(smem_raw + L::gl_off);
+    double *s_gms = s_gma + 256;
     float *s_win = reinterpret_cast<float *>(smem_raw + L::win_off(kp.nr, kp.rr_shared));
     const int n_win = FLU == PMO_FLU_SHARED ? kp.win_dim[0] * kp.win_dim[1] * kp.win_dim[2] : 0;
+    const bool fd = GRAD && kp.fd_n > 0;
+    double *s_fdsum = reinterpret_cast<double *>(
+        smem_raw + L::total(kp.nr, kp.rr_shared, FLU, kp.win_dim));
+    float *s_fdL = reinterpret_cast<float *>(s_fdsum + 2 * PMO_FD_MAX) +
+                   threadIdx.x * 2 * PMO_FD_MAX;   // this thread's sum of mu * L per target
+    float *s_fdN = s_fdL + PMO_FD_MAX;             // and interaction count per target
 
     // ---- block set-up: property table, zeroed privatised tallies ----
     for (int i = threadIdx.x; i < 256; i += blockDim.x) {
@@ -127,6 +167,10 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
         s_valid[i] = ok ? 1 : 0;
     }
     for (int i = threadIdx.x; i < PMO_LEDGER_N; i += blockDim.x) s_led[i] = 0.0;
+    if (GRAD)
+        for (int i = threadIdx.x; i < 512; i += blockDim.x) s_gma[i] = 0.0;
+    if (fd)
+        for (int i = threadIdx.x; i < 2 * PMO_FD_MAX; i += blockDim.x) s_fdsum[i] = 0.0;
     for (int i = threadIdx.x; i < PMO_COUNTERS_N; i += blockDim.x) s_cnt[i] = 0ull;
     if (kp.rr_shared)
         for (int i = threadIdx.x; i < PMO_RR_CATS * kp.nr; i += blockDim.x) s_rr[i] = R(0);
@@ -143,6 +187,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
     const uint64_t N = kp.count;
     const bool export_exits = (kp.flags & PMO_FLAG_EXPORT_EXITS) != 0;
     const bool photon_stats = (kp.flags & PMO_FLAG_PHOTON_STATS) != 0;
+    const bool score_record = !GRAD && (kp.flags & PMO_FLAG_SCORE_RECORD) != 0;
 
     // thread totals, reduced once at the end
     double t_abs = 0.0;
@@ -158,6 +203,11 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
     R hw = 0;
     R mt = 0, imt = 0, ma_mt = 0, ni = 1;
     uint32_t k = 0, f = 0, ncr = 0;
+    int ecode = -1;                 // exit bin code (category * nr + bin), -1: none
+    // gradient replay: q of the photon, path length and sum of 1/mu_s over
+    // interactions in the current cell, 1/mu_s of the cell
+    float gq = 0.f, gL = 0.f, gN = 0.f, gC = 0.f;
+    R ims = 0;
     uint32_t pend_lin = 0xffffffffu;
     float pend_w = 0.f;
 
@@ -169,7 +219,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
     // offset of the voxel holding the photon from the box centre, in voxels
     auto box_k = [&](R q) -> int {
         const int m = rad - 1;
-        int k = (int)rint(q * inv_l);
+        int k = (int)rint(xmul(q, inv_l));
         return k < -m ? -m : (k > m ? m : k);
     };
     auto deposit = [&](float dw) {
@@ -207,25 +257,55 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
         }
     };
     auto set_dir_inverse = [&]() {
-        ivx = R(1) / vx;
-        ivy = R(1) / vy;
-        ivz = R(1) / vz;
+        ivx = xdiv(R(1), vx);
+        ivy = xdiv(R(1), vy);
+        ivz = xdiv(R(1), vz);
     };
     auto load_props = [&]() {
         if (PROPS == PMO_PROPS_VOXEL) {
             const float a = __ldg(kp.vox_ma + lin), s = __ldg(kp.vox_ms + lin);
-            mt = (R)a + (R)s;
-            imt = mt > R(0) ? R(1) / mt : R(0);
-            ma_mt = mt > R(0) ? (R)a / mt : R(0);
+            mt = xadd((R)a, (R)s);
+            imt = mt > R(0) ? xdiv(R(1), mt) : R(0);
+            ma_mt = mt > R(0) ? xdiv((R)a, mt) : R(0);
+            if (GRAD) ims = s > 0.f ? xdiv(R(1), (R)s) : R(0);
         } else {
             mt = s_tab[lab].mt;
             imt = s_tab[lab].imt;
             ma_mt = s_tab[lab].ma_mt;
+            if (GRAD) ims = s_tab[lab].ims;
+        }
+    };
+    // gradient replay: hand the current cell's path length and 1/mu_s sum to
+    // the per-voxel grids and the per-label sums
+    auto grad_flush = [&]() {
+        if (GRAD && fd && (gL != 0.f || gC != 0.f)) {
+            const int t = __ldg(kp.fd_target + lin);
+            if (t >= 0 && t < kp.fd_n) {
+                const float mu_a = (float)xmul(ma_mt, mt);
+                const float mu = kp.fd_param == 0 ? mu_a : (float)mt - mu_a;
+                s_fdL[t] += mu * gL;
+                s_fdN[t] += gC;
+            }
+            gC = 0.f;
+        }
+        if (GRAD && (gL != 0.f || gN != 0.f)) {
+            const float dma = -gq * gL;
+            const float dms = gq * gN - gq * gL;
+            if (kp.d_ma_voxel) {
+                atomicAdd(kp.d_ma_voxel + lin, dma);
+                atomicAdd(kp.d_ms_voxel + lin, dms);
+            }
+            atomicAdd(s_gma + lab, (double)dma);
+            atomicAdd(s_gms + lab, (double)dms);
+            gL = 0.f;
+            gN = 0.f;
         }
     };
     // photon end: per-photon outputs and counters
     auto finish = [&]() {
         if (FLU != PMO_FLU_NONE) deposit_flush();
+        // a replayed photon that ends without a binned exit left the forward path
+        if (GRAD && ecode < 0) atomicAdd(kp.gcounters + PMO_G_MISMATCH, 1ull);
         const uint64_t j = pid - kp.begin;
         if (export_exits) {
             kp.exit_add[j] = ix;
@@ -238,6 +318,10 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             kp.exit_v[N + j] = (float)vy;
             kp.exit_v[2 * N + j] = (float)vz;
             kp.exit_w[j] = (float)w;
+        }
+        if (score_record) {
+            kp.score_bin[j] = ecode;
+            kp.score_w[j] = (float)w;
         }
         if (photon_stats) {
             kp.ph_interact[j] = k;
@@ -259,28 +343,56 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
     // encoded exit position (:302-310, pymopt/metrics/_scoring.py:16-25)
     auto exit_tally = [&](int ax) {
         const double wd = (double)w;
-        atomicAdd(s_led + (vz < R(0) ? PMO_L_RD : (vz > R(0) ? PMO_L_TT : PMO_L_EXIT0)), wd);
+        if (!GRAD)
+            atomicAdd(s_led + (vz < R(0) ? PMO_L_RD : (vz > R(0) ? PMO_L_TT : PMO_L_EXIT0)), wd);
         int cat = -1;
         if (ax == 2) {
             cat = vz < R(0) ? PMO_RR_TOP : PMO_RR_BOTTOM;
-            atomicAdd(s_led + (vz < R(0) ? PMO_L_RD_TOP : PMO_L_TT_BOTTOM), wd);
+            if (!GRAD) atomicAdd(s_led + (vz < R(0) ? PMO_L_RD_TOP : PMO_L_TT_BOTTOM), wd);
         } else if (vz < R(0)) {
             cat = PMO_RR_LAT_NEG;
         } else if (vz > R(0)) {
             cat = PMO_RR_LAT_POS;
         }
         if (cat >= 0 && kp.nr > 0) {
-            const R x = l * (R)(ix - kp.cx) + px;
-            const R y = l * (R)(iy - kp.cy) + py;
-            const R r = psqrt(x * x + y * y);
+            const R x = xfma(l, (R)(ix - kp.cx), px);
+            const R y = xfma(l, (R)(iy - kp.cy), py);
+            const R r = psqrt(xfma(y, y, xmul(x, x)));
             if (r > R(0)) {
-                const R q = ceil(r / (R)kp.dr);
+                const R q = ceil(xdiv(r, (R)kp.dr));
                 if (q >= R(1) && q <= (R)kp.nr) {
                     const int b = (int)q - 1;
-                    if (kp.rr_shared)
+                    ecode = cat * kp.nr + b;
+                    if (GRAD) {
+                    } else if (kp.rr_shared) {
                         atomicAdd(s_rr + cat * kp.nr + b, (R)w);
-                    else
+                    } else {
                         atomicAdd(kp.rr + cat * kp.nr + b, (float)w);
+                    }
+                }
+            }
+        }
+        if (GRAD) {
+            // the replay must end where the forward run did
+            const uint64_t jr = pid - kp.begin;
+            if (ecode != kp.score_bin[jr] || (float)w != kp.score_w[jr])
+                atomicAdd(kp.gcounters + PMO_G_MISMATCH, 1ull);
+            if (fd) {
+                // reweight this photon for mu * (1 +- h) in each target it crossed
+                const float h = kp.fd_h;
+                for (int t = 0; t < kp.fd_n; ++t) {
+                    const float A = s_fdL[t], n = s_fdN[t];
+                    if (A == 0.f && n == 0.f) continue;
+                    float ep, em;
+                    if (kp.fd_param == 0) {
+                        ep = expm1f(-h * A);
+                        em = expm1f(h * A);
+                    } else {
+                        ep = expm1f(n * log1pf(h) - h * A);
+                        em = expm1f(n * log1pf(-h) + h * A);
+                    }
+                    atomicAdd(s_fdsum + 2 * t, (double)gq * (double)ep);
+                    atomicAdd(s_fdsum + 2 * t + 1, (double)gq * (double)em);
                 }
             }
         }
@@ -292,6 +404,19 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
     auto start = [&](uint64_t jj) -> bool {
         pid = kp.begin + jj;
         k = f = ncr = 0;
+        ecode = -1;
+        if (GRAD) {
+            const int code = kp.score_bin[jj];
+            gq = code >= 0 ? __ldg(kp.coef + code) * kp.score_w[jj] : 0.f;
+            gL = gN = gC = 0.f;
+            if (fd)
+                for (int t = 0; t < kp.fd_n; ++t) s_fdL[t] = s_fdN[t] = 0.f;
+            if (gq == 0.f) {
+                atomicAdd(kp.gcounters + PMO_G_SKIPPED, 1ull);
+                return false;
+            }
+            atomicAdd(kp.gcounters + PMO_G_REPLAYED, 1ull);
+        }
         if (kp.source == PMO_SRC_STATE) {
             ix = kp.state_add[jj];
             iy = kp.state_add[N + jj];
@@ -320,15 +445,15 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
                     // x, y ~ N(0, sigma) (gaussianBeam, :267-287) by Box-Muller,
                     // split into voxel index + offset in [-l/2, l/2] (:242-252)
                     const R u0 = u01<R>(rs.x), u1 = u01<R>(rs.y);
-                    const R rad = (R)kp.beam_sigma * psqrt(-2 * plog(u0));
+                    const R rad = xmul((R)kp.beam_sigma, psqrt(xmul(R(2), pneglog(u0))));
                     R sn, cs;
                     psincos2pi(u1, &sn, &cs);
-                    const R xy[2] = {rad * cs, rad * sn};
+                    const R xy[2] = {xmul(rad, cs), xmul(rad, sn)};
 #pragma unroll
                     for (int a = 0; a < 2; ++a) {
-                        const R fl = floor(xy[a] / l);
-                        R off = xy[a] - (fl + R(0.5)) * l;
-                        if (fabs(off) >= hl) off = sgn(off) * hl;
+                        const R fl = floor(xdiv(xy[a], l));
+                        R off = xfma(-xadd(fl, R(0.5)), l, xy[a]);
+                        if (fabs(off) >= hl) off = copysign(hl, off);
                         if (a == 0) { ix += (int)fl; px = off; }
                         else { iy += (int)fl; py = off; }
                     }
@@ -363,7 +488,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             lab = __ldg(kp.labels + lin);
             rad = 1;
         }
-        hw = (R)rad * l - hl;
+        hw = xfma((R)rad, l, -hl);
         if (!s_valid[lab]) {
             fail(PMO_C_ERR_LABEL);
             return false;
@@ -380,37 +505,39 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
     auto cycle = [&]() -> bool {
         const uint4 rn = philox4x32_10(make_uint4(k, 0u, (uint32_t)pid, (uint32_t)(pid >> 32)), key);
         ++k;
-        R st = -plog(u01<R>(rn.x));  // step in optical depths (:75)
+        R st = pneglog(u01<R>(rn.x));  // step in optical depths (:75)
 
         for (;;) {
             // distance to the nearest face; db starts at 1000 (:80-90)
-            const R dx = (copysign(hw, vx) - px) * ivx;
-            const R dy = (copysign(hw, vy) - py) * ivy;
-            const R dz = (copysign(hw, vz) - pz) * ivz;
+            const R dx = xmul(xsub(copysign(hw, vx), px), ivx);
+            const R dy = xmul(xsub(copysign(hw, vy), py), ivy);
+            const R dz = xmul(xsub(copysign(hw, vz), pz), ivz);
             R db = R(1000);
             int ax = 0;
             if (dx < db) { db = dx; ax = 0; }
             if (dy < db) { db = dy; ax = 1; }
             if (dz < db) { db = dz; ax = 2; }
-            const R dbmt = db * mt;
+            const R dbmt = xmul(db, mt);
             if (!(st >= dbmt)) {
                 // hop inside the voxel (:170-175)
-                const R s = st * imt;
-                px += vx * s;
-                py += vy * s;
-                pz += vz * s;
+                const R s = xmul(st, imt);
+                px = xfma(vx, s, px);
+                py = xfma(vy, s, py);
+                pz = xfma(vz, s, pz);
+                if (GRAD) gL += (float)s;
                 break;
             }
             // move to the face and snap (:92-96)
-            px += vx * db;
-            py += vy * db;
-            pz += vz * db;
+            px = xfma(vx, db, px);
+            py = xfma(vy, db, py);
+            pz = xfma(vz, db, pz);
+            if (GRAD) gL += (float)db;
             const R va = ax == 0 ? vx : (ax == 1 ? vy : vz);
             const R face = copysign(hw, va);
             if (ax == 0) px = face;
             else if (ax == 1) py = face;
             else pz = face;
-            st -= dbmt;
+            st = xsub(st, dbmt);
             ++ncr;
             if (ncr + k - 1 > cap) { fail(PMO_C_ERR_CAP); return false; }
             const bool neg = signbit(va);
@@ -424,9 +551,9 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
                 const int kx = ax == 0 ? m : box_k(px);
                 const int ky = ax == 1 ? m : box_k(py);
                 const int kz = ax == 2 ? m : box_k(pz);
-                fx = ax == 0 ? copysign(hl, va) : px - (R)kx * l;
-                fy = ax == 1 ? copysign(hl, va) : py - (R)ky * l;
-                fz = ax == 2 ? copysign(hl, va) : pz - (R)kz * l;
+                fx = ax == 0 ? copysign(hl, va) : xfma(-(R)kx, l, px);
+                fy = ax == 1 ? copysign(hl, va) : xfma(-(R)ky, l, py);
+                fz = ax == 2 ? copysign(hl, va) : xfma(-(R)kz, l, pz);
                 cx += kx;
                 cy += ky;
                 cz += kz;
@@ -453,6 +580,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             }
             // step into the neighbour voxel and take its box (:137-148)
             auto enter = [&]() {
+                grad_flush();
                 ix = ax == 0 ? nc : cx;
                 iy = ax == 1 ? nc : cy;
                 iz = ax == 2 ? nc : cz;
@@ -461,7 +589,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
                 pz = ax == 2 ? -fz : fz;
                 lin = nlin;
                 rad = nrad;
-                hw = (R)rad * l - hl;
+                hw = xfma((R)rad, l, -hl);
             };
             if (PROPS == PMO_PROPS_LABEL && nlab == lab) {
                 // same label on the other side: same n and mu (:154-167)
@@ -478,22 +606,27 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
                 const R u = u01<R>(fr.x);
                 R ca = fabs(va);
                 if (ca > R(1)) ca = R(1);
-                const R nr = ni / nt;
-                const R sa = psqrt(1 - ca * ca);
-                const R sb = nr * sa;
+                const R nr = xdiv(ni, nt);
+                const R sa = psqrt(xfma(-ca, ca, R(1)));
+                const R sb = xmul(nr, sa);
                 R ra, cb = R(1);
                 if (ni > nt && sb >= R(1)) {
                     ra = R(1);  // TIR
                 } else {
-                    cb = psqrt(1 - sb * sb);
+                    cb = psqrt(xfma(-sb, sb, R(1)));
                     if (ca == R(1)) {
                         ra = R(0);  // ai == 0 (:113-120)
                     } else {
-                        const R cap_ = ca * cb - sa * sb;
-                        const R cam = ca * cb + sa * sb;
-                        const R sap = sa * cb + ca * sb;
-                        const R sam = sa * cb - ca * sb;
-                        ra = R(0.5) * sam * sam * (cam * cam + cap_ * cap_) / (sap * sap * cam * cam);
+                        const R cacb = xmul(ca, cb), sasb = xmul(sa, sb);
+                        const R sacb = xmul(sa, cb), casb = xmul(ca, sb);
+                        const R cap_ = xsub(cacb, sasb);   // cos(ai + at)
+                        const R cam = xadd(cacb, sasb);    // cos(ai - at)
+                        const R sap = xadd(sacb, casb);    // sin(ai + at)
+                        const R sam = xsub(sacb, casb);    // sin(ai - at)
+                        const R num = xmul(xmul(xmul(R(0.5), sam), sam),
+                                           xfma(cap_, cap_, xmul(cam, cam)));
+                        const R den = xmul(xmul(xmul(sap, sap), cam), cam);
+                        ra = xdiv(num, den);
                     }
                 }
                 if (!(ra < u)) {
@@ -505,13 +638,13 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
                     continue;
                 }
                 // refract: tangential * ni/nt, normal = sign * cos(at) (:124-134)
-                vx = ax == 0 ? sgn(vx) * cb : vx * nr;
-                vy = ax == 1 ? sgn(vy) * cb : vy * nr;
-                vz = ax == 2 ? sgn(vz) * cb : vz * nr;
-                const R inv = pinvnorm(vx * vx + vy * vy + vz * vz);
-                vx *= inv;
-                vy *= inv;
-                vz *= inv;
+                vx = ax == 0 ? xmul(sgn(vx), cb) : xmul(vx, nr);
+                vy = ax == 1 ? xmul(sgn(vy), cb) : xmul(vy, nr);
+                vz = ax == 2 ? xmul(sgn(vz), cb) : xmul(vz, nr);
+                const R inv = pinvnorm(sumsq(vx, vy, vz));
+                vx = xmul(vx, inv);
+                vy = xmul(vy, inv);
+                vz = xmul(vz, inv);
                 set_dir_inverse();
             }
             // cross (:137-148)
@@ -526,9 +659,13 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             load_props();
         }
 
+        if (GRAD) {
+            gN += (float)ims;
+            gC += 1.f;
+        }
         // absorption by implicit capture (:179)
         {
-            const R wn = w - w * ma_mt;
+            const R wn = xfma(-w, ma_mt, w);
             const double dw = (double)w - (double)wn;
             w = wn;
             t_abs += dw;
@@ -546,34 +683,36 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
                 finish();
                 return false;
             }
-            const R wn = w * 10;
+            const R wn = xmul(w, R(10));
             atomicAdd(s_led + PMO_L_RGAIN, (double)wn - (double)w);
             w = wn;
         }
         // scattering: HG polar angle, uniform azimuth, rotation (:197-219)
         {
             const R ct = hg_cos<R>(s_tab[lab], u01<R>(rn.z));
-            const R s2 = 1 - ct * ct;
+            const R s2 = xfma(-ct, ct, R(1));
             const R sth = psqrt(s2 > R(0) ? s2 : R(0));
             R sf, cf;
             psincos2pi(u01<R>(rn.w), &sf, &cf);
             if (R(0.99999) < fabs(vz)) {
                 const R sz = sgn(vz);
-                vx = sth * cf;
-                vy = sth * sf;
-                vz = sz * ct;
+                vx = xmul(sth, cf);
+                vy = xmul(sth, sf);
+                vz = xmul(sz, ct);
             } else {
-                const R tmp = psqrt(1 - vz * vz);
-                const R fct = sth / tmp;
+                const R tmp = psqrt(xfma(-vz, vz, R(1)));
+                const R fct = xdiv(sth, tmp);
                 const R ox = vx, oy = vy, oz = vz;
-                vx = fct * (ox * oz * cf - oy * sf) + ox * ct;
-                vy = fct * (oy * oz * cf + ox * sf) + oy * ct;
-                vz = -sth * cf * tmp + oz * ct;
+                const R tx = xsub(xmul(xmul(ox, oz), cf), xmul(oy, sf));
+                const R ty = xadd(xmul(xmul(oy, oz), cf), xmul(ox, sf));
+                vx = xfma(fct, tx, xmul(ox, ct));
+                vy = xfma(fct, ty, xmul(oy, ct));
+                vz = xfma(xmul(-sth, cf), tmp, xmul(oz, ct));
             }
-            const R inv = pinvnorm(vx * vx + vy * vy + vz * vz);
-            vx *= inv;
-            vy *= inv;
-            vz *= inv;
+            const R inv = pinvnorm(sumsq(vx, vy, vz));
+            vx = xmul(vx, inv);
+            vy = xmul(vy, inv);
+            vz = xmul(vz, inv);
             set_dir_inverse();
         }
         if (ncr + k > cap) { fail(PMO_C_ERR_CAP); return false; }
@@ -627,6 +766,15 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
     if (kp.rr_shared)
         for (int i = threadIdx.x; i < PMO_RR_CATS * kp.nr; i += blockDim.x)
             if (s_rr[i] != R(0)) atomicAdd(kp.rr + i, (float)s_rr[i]);
+    if (fd)
+        for (int i = threadIdx.x; i < 2 * kp.fd_n; i += blockDim.x)
+            if (s_fdsum[i] != 0.0) atomicAdd(kp.fd_out + i, s_fdsum[i]);
+    if (GRAD) {
+        for (int i = threadIdx.x; i < kp.n_labels; i += blockDim.x) {
+            if (kp.d_ma_label && s_gma[i] != 0.0) atomicAdd(kp.d_ma_label + i, s_gma[i]);
+            if (kp.d_ms_label && s_gms[i] != 0.0) atomicAdd(kp.d_ms_label + i, s_gms[i]);
+        }
+    }
     if (FLU == PMO_FLU_SHARED) {
         const int wy = kp.win_dim[1], wz = kp.win_dim[2];
         for (int i = threadIdx.x; i < n_win; i += blockDim.x) {
