@@ -256,6 +256,86 @@ int pmo_run_plain(const pmo_problem *prob, const pmo_tallies *tal,
 int pmo_run_grad(const pmo_problem *prob, const pmo_grad *grad, const pmo_launch *launch,
                  void *workspace, size_t workspace_bytes, void *stream);
 
+/* ---- batched slab problems ------------------------------------------- */
+
+/* One laterally infinite single-layer slab: the geometry of a PlateModel with
+   one layer (pymopt/voxel_gpu/_classes.py:396-459) when x_size, y_size grow
+   without bound.  Photons enter at the origin of the top face along +z with
+   weight w0 = 1 - Rsp (pymopt/voxel_gpu/_classes.py:204-221). */
+typedef struct pmo_slab {
+    float ma, ms, g;              /* mu_a, mu_s [1/mm], anisotropy */
+    float n_tissue, n_ambient;    /* refractive indices inside / outside */
+    float thickness;              /* [mm] */
+    float dr;                     /* R(r) bin width [mm] */
+    uint32_t photons;             /* photon budget */
+} pmo_slab;
+
+/* A work item: photons [begin, begin + count) of one problem. */
+typedef struct pmo_batch_item {
+    uint32_t problem, begin, count;
+} pmo_batch_item;
+
+/* Per-problem raw sums (double), accumulated by pmo_run_batched. */
+#define PMO_BS_RD      0          /* sum w of exits through the top face       */
+#define PMO_BS_RD_L    1          /* sum w * L (path length)                   */
+#define PMO_BS_RD_N    2          /* sum w * n (interactions)                  */
+#define PMO_BS_TT      3          /* bottom face                               */
+#define PMO_BS_TT_L    4
+#define PMO_BS_TT_N    5
+#define PMO_BS_ABS     6          /* absorbed weight                           */
+#define PMO_BS_WINIT   7          /* launched weight                           */
+#define PMO_BS_RGAIN   8
+#define PMO_BS_RLOSS   9
+#define PMO_BS_ERRW    10
+#define PMO_BS_INTER   11         /* interactions (count)                      */
+#define PMO_BS_N       16
+
+/* Per-problem results of pmo_batch_finalize (double): */
+#define PMO_BR_RD        0        /* Rd                                        */
+#define PMO_BR_TT        1        /* Tt                                        */
+#define PMO_BR_A         2        /* absorbed fraction                         */
+#define PMO_BR_DRD_DMA   3        /* dRd/dmu_a = -E[w L 1_top]                 */
+#define PMO_BR_DRD_DMS   4        /* dRd/dmu_s = E[w (n/mu_s - L) 1_top]       */
+#define PMO_BR_DTT_DMA   5
+#define PMO_BR_DTT_DMS   6
+#define PMO_BR_BALANCE   7        /* energy ledger residual / launched weight  */
+#define PMO_BR_N         8
+
+typedef struct pmo_batch {
+    const pmo_slab *slabs;        /* device array of n_problems */
+    int32_t n_problems;
+    const pmo_batch_item *items;  /* device work queue of n_items, in order */
+    int32_t n_items;
+    uint64_t seed;
+    int32_t nr;                   /* R(r) bins per problem */
+    double *sums;                 /* n_problems * PMO_BS_N, accumulated */
+    float *bins;                  /* n_problems * nr * 3: sum w, w L, w n of
+                                     top exits in (i dr, (i+1) dr] */
+    uint32_t *remaining;          /* per problem photons still in flight (set
+                                     to the budget by the caller) or NULL */
+    unsigned long long *t_done;   /* per problem completion time (ns, device
+                                     global timer) or NULL */
+    int32_t precision;            /* PMO_FP32 or PMO_FP64 */
+    uint32_t max_events;          /* 0 = 2^26 */
+} pmo_batch;
+
+/*
+ * Run every work item in one persistent launch: forward transport and the
+ * perturbation Monte Carlo derivatives of Rd, Tt and R(r) with respect to
+ * mu_a and mu_s, in the same pass (single layer, so the per-photon path
+ * length and interaction count suffice).  Photon j of problem p draws from
+ * Philox with counter (n, stream + 4 p, j, 0): problem 0 has the streams of
+ * pmo_run_plain.  No counterpart in the reference, which runs one problem
+ * per launch.
+ */
+int pmo_run_batched(const pmo_batch *batch, const pmo_launch *launch, void *workspace,
+                    size_t workspace_bytes, void *stream);
+
+/* Per-problem results (n_problems * PMO_BR_N doubles) and normalised R(r)
+   with its derivatives (n_problems * nr * 3 doubles: R, dR/dmu_a, dR/dmu_s,
+   [1/mm^2]) from the sums of pmo_run_batched. */
+int pmo_batch_finalize(const pmo_batch *batch, double *results, double *rr, void *stream);
+
 /*
  * pmo_run_plain without a caller-allocated workspace.  No counterpart in the
  * reference.  For callers that cannot allocate device memory themselves (a

@@ -162,5 +162,35 @@ class PmoGrad(C.Structure):
     ]
 
 
+PMO_BS_RD, PMO_BS_RD_L, PMO_BS_RD_N, PMO_BS_TT, PMO_BS_TT_L, PMO_BS_TT_N = 0, 1, 2, 3, 4, 5
+PMO_BS_ABS, PMO_BS_WINIT, PMO_BS_RGAIN, PMO_BS_RLOSS, PMO_BS_ERRW, PMO_BS_INTER = 6, 7, 8, 9, 10, 11
+PMO_BS_N = 16
+PMO_BR_RD, PMO_BR_TT, PMO_BR_A = 0, 1, 2
+PMO_BR_DRD_DMA, PMO_BR_DRD_DMS, PMO_BR_DTT_DMA, PMO_BR_DTT_DMS = 3, 4, 5, 6
+PMO_BR_BALANCE = 7
+PMO_BR_N = 8
+
+
+class PmoSlab(C.Structure):
+    _fields_ = [("ma", C.c_float), ("ms", C.c_float), ("g", C.c_float),
+                ("n_tissue", C.c_float), ("n_ambient", C.c_float), ("thickness", C.c_float),
+                ("dr", C.c_float), ("photons", C.c_uint32)]
+
+
+class PmoBatchItem(C.Structure):
+    _fields_ = [("problem", C.c_uint32), ("begin", C.c_uint32), ("count", C.c_uint32)]
+
+
+class PmoBatch(C.Structure):
+    _fields_ = [
+        ("slabs", C.c_void_p), ("n_problems", C.c_int32),
+        ("items", C.c_void_p), ("n_items", C.c_int32),
+        ("seed", C.c_uint64), ("nr", C.c_int32),
+        ("sums", C.c_void_p), ("bins", C.c_void_p),
+        ("remaining", C.c_void_p), ("t_done", C.c_void_p),
+        ("precision", C.c_int32), ("max_events", C.c_uint32),
+    ]
+
+
 class PmoLaunch(C.Structure):
     _fields_ = [("block_threads", C.c_int32), ("blocks_per_sm", C.c_int32)]

@@ -1,0 +1,324 @@
+"""Thousands of independent slab problems in one persistent launch.
+
+:class:`SlabBatch` runs a batch of laterally infinite single-layer slabs (the
+reference's one-layer PlateModel with x_size, y_size taken to infinity,
+pymopt/voxel_gpu/_classes.py:396-459) through ``pmo_run_batched``: one
+persistent kernel drains a device work queue of (problem, photon range)
+items, computing in the same pass Rd, Tt, A, R(r) and their perturbation
+Monte Carlo derivatives with respect to mu_a and mu_s.  The launch sequence
+(clearing the sums, the kernel, the FP64 finalisation) is captured in a CUDA
+graph and replayed.
+
+The launch shape (threads per block, photons per work item) is chosen by a
+small autotuner that times candidate shapes on a down-scaled copy of the
+batch and caches the winner per device and batch signature.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import time
+from typing import Optional
+
+import numpy as np
+import torch
+
+from . import _abi as A
+from . import engine as E
+from ._lib import check, load
+
+SLAB_DTYPE = np.dtype([("ma", "<f4"), ("ms", "<f4"), ("g", "<f4"), ("n_tissue", "<f4"),
+                       ("n_ambient", "<f4"), ("thickness", "<f4"), ("dr", "<f4"),
+                       ("photons", "<u4")])
+ITEM_DTYPE = np.dtype([("problem", "<u4"), ("begin", "<u4"), ("count", "<u4")])
+
+_TUNE_CACHE: dict = {}
+
+
+def build_items(photons: np.ndarray, chunk: int, order: Optional[np.ndarray] = None) -> np.ndarray:
+    """Work queue: each problem's photons in chunks of ``chunk``, problems in
+    ``order`` (default: ascending budget, so small problems finish early)."""
+    photons = np.asarray(photons, np.int64)
+    if order is None:
+        order = np.argsort(photons, kind="stable")
+    counts = (photons[order] + chunk - 1) // chunk
+    items = np.empty(int(counts.sum()), ITEM_DTYPE)
+    prob = np.repeat(order, counts)
+    first = np.repeat(np.cumsum(counts) - counts, counts)
+    k = np.arange(items.size) - first
+    items["problem"] = prob
+    items["begin"] = k * chunk
+    items["count"] = np.minimum(chunk, photons[prob] - k * chunk)
+    return items
+
+
+class SlabBatch:
+    """A batch of slab problems resident on one GPU.
+
+    Parameters are arrays of equal length: ``ma``, ``ms`` [1/mm], ``g``, ``n``
+    (tissue index), ``thickness`` [mm], ``photons`` (budget per problem).
+    ``dr`` [mm] and ``nr`` set the R(r) bins of every problem.
+    """
+
+    def __init__(self, ma, ms, g, n, thickness, photons, *, n_ambient=1.0, nr: int = 32,
+                 dr=0.1, seed: int = 0, precision: int = A.PMO_FP32, device=None,
+                 block_threads: int = 0, chunk: int = 0, autotune: bool = True):
+        load()
+        self.device = E.require_cuda(device)
+        P = len(ma)
+        slabs = np.zeros(P, SLAB_DTYPE)
+        slabs["ma"], slabs["ms"], slabs["g"] = ma, ms, g
+        slabs["n_tissue"] = n
+        slabs["n_ambient"] = n_ambient
+        slabs["thickness"] = thickness
+        slabs["dr"] = dr
+        slabs["photons"] = photons
+        if np.any(slabs["thickness"] <= 0) or np.any(slabs["ma"] < 0) or np.any(slabs["ms"] < 0):
+            raise ValueError("thickness must be positive and ma, ms non-negative")
+        if np.any(slabs["photons"] < 1) or np.any(np.abs(slabs["g"]) > 1):
+            raise ValueError("photon budgets must be >= 1 and |g| <= 1")
+        self.host_slabs = slabs
+        self.P = P
+        self.nr = int(nr)
+        self.seed = int(seed)
+        self.precision = precision
+        dev = self.device
+        self.slabs = torch.from_numpy(slabs.view(np.uint8).copy()).to(dev)
+        self.sums = torch.zeros(P, A.PMO_BS_N, dtype=torch.float64, device=dev)
+        self.bins = torch.zeros(P, max(self.nr, 1), 3, dtype=torch.float32, device=dev)
+        self.remaining = torch.zeros(P, dtype=torch.int32, device=dev)
+        self.budget = torch.from_numpy(slabs["photons"].astype(np.int32)).to(dev)
+        self.t_done = torch.zeros(P, dtype=torch.int64, device=dev)
+        self.results = torch.zeros(P, A.PMO_BR_N, dtype=torch.float64, device=dev)
+        self.rr = torch.zeros(P, max(self.nr, 1), 3, dtype=torch.float64, device=dev)
+        self.workspace = torch.zeros(int(load().pmo_workspace_bytes()), dtype=torch.uint8,
+                                     device=dev)
+        self.graph = None
+        if autotune and not (block_threads and chunk):
+            block_threads, chunk = self.autotune()
+        self.block_threads = block_threads or 128
+        self.set_chunk(chunk or 256)
+
+    # ------------------------------------------------------------------
+    def set_chunk(self, chunk: int) -> None:
+        self.chunk = int(chunk)
+        items = build_items(self.host_slabs["photons"], self.chunk)
+        self.items = torch.from_numpy(items.view(np.uint8).copy()).to(self.device)
+        self.n_items = len(items)
+        self.graph = None
+
+    def _struct(self, slabs=None, items=None, n_items=None, sums=None, bins=None,
+                remaining=None, t_done=None, P=None) -> A.PmoBatch:
+        b = A.PmoBatch()
+        b.slabs = (slabs if slabs is not None else self.slabs).data_ptr()
+        b.n_problems = P or self.P
+        b.items = (items if items is not None else self.items).data_ptr()
+        b.n_items = n_items if n_items is not None else self.n_items
+        b.seed = self.seed & 0xFFFFFFFFFFFFFFFF
+        b.nr = self.nr
+        b.sums = (sums if sums is not None else self.sums).data_ptr()
+        b.bins = (bins if bins is not None else self.bins).data_ptr()
+        b.remaining = (remaining if remaining is not None else self.remaining).data_ptr()
+        b.t_done = (t_done if t_done is not None else self.t_done).data_ptr()
+        b.precision = self.precision
+        return b
+
+    def launch(self, stream=None) -> None:
+        """Enqueue one evaluation: clear sums, run the batch, finalise."""
+        self.sums.zero_()
+        self.bins.zero_()
+        self.remaining.copy_(self.budget)
+        self.t_done.zero_()
+        b = self._struct()
+        lib = load()
+        st = lib.pmo_run_batched(C.byref(b), C.byref(A.PmoLaunch(self.block_threads, 0)),
+                                 C.c_void_p(self.workspace.data_ptr()), self.workspace.numel(),
+                                 E._stream_handle(stream))
+        check(st, "pmo_run_batched")
+        st = lib.pmo_batch_finalize(C.byref(b), C.c_void_p(self.results.data_ptr()),
+                                    C.c_void_p(self.rr.data_ptr()) if self.nr > 0 else None,
+                                    E._stream_handle(stream))
+        check(st, "pmo_batch_finalize")
+
+    def capture(self) -> "torch.cuda.CUDAGraph":
+        """Capture :meth:`launch` in a CUDA graph (warms up once first)."""
+        s = torch.cuda.Stream(device=self.device)
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            self.launch()
+        torch.cuda.current_stream().wait_stream(s)
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.launch()
+        self.graph = g
+        return g
+
+    def run(self, use_graph: bool = True) -> dict:
+        """One evaluation; returns host results (synchronises)."""
+        if use_graph:
+            if self.graph is None:
+                self.capture()
+            self.graph.replay()
+        else:
+            self.launch()
+        return self.fetch()
+
+    def fetch(self) -> dict:
+        res = self.results.cpu().numpy()
+        rr = self.rr.cpu().numpy()
+        ws = self.workspace[8:16].cpu().numpy().view(np.uint64)[0]
+        td = self.t_done.cpu().numpy().view(np.uint64)
+        done_ms = (td.astype(np.float64) - float(ws)) / 1e6
+        return {
+            "Rd": res[:, A.PMO_BR_RD], "Tt": res[:, A.PMO_BR_TT], "A": res[:, A.PMO_BR_A],
+            "dRd_dma": res[:, A.PMO_BR_DRD_DMA], "dRd_dms": res[:, A.PMO_BR_DRD_DMS],
+            "dTt_dma": res[:, A.PMO_BR_DTT_DMA], "dTt_dms": res[:, A.PMO_BR_DTT_DMS],
+            "balance": res[:, A.PMO_BR_BALANCE],
+            "Rr": rr[:, :, 0], "dRr_dma": rr[:, :, 1], "dRr_dms": rr[:, :, 2],
+            "completion_ms": done_ms,
+            "sums": self.sums.cpu().numpy(),
+        }
+
+    # ------------------------------------------------------------------
+    def autotune(self, candidates=None, scale: float = 1 / 64) -> tuple:
+        """Pick (threads per block, photons per work item) by timing each
+        candidate on the batch with every budget scaled by ``scale``."""
+        sig = (torch.cuda.get_device_name(self.device), self.P,
+               int(self.host_slabs["photons"].sum()), round(float(self.host_slabs["ma"].mean()), 6))
+        if sig in _TUNE_CACHE:
+            return _TUNE_CACHE[sig]
+        if candidates is None:
+            candidates = [(t, c) for t in (64, 128, 256) for c in (64, 512, 4096)]
+        dev = self.device
+        small = self.host_slabs.copy()
+        small["photons"] = np.maximum(1, (small["photons"] * scale).astype(np.int64))
+        slabs = torch.from_numpy(small.view(np.uint8).copy()).to(dev)
+        sums = torch.zeros_like(self.sums)
+        bins = torch.zeros_like(self.bins)
+        rem = torch.zeros_like(self.remaining)
+        tdone = torch.zeros_like(self.t_done)
+        lib = load()
+        best, best_t = None, float("inf")
+        for threads, chunk in candidates:
+            items = build_items(small["photons"], chunk)
+            d_items = torch.from_numpy(items.view(np.uint8).copy()).to(dev)
+            b = self._struct(slabs=slabs, items=d_items, n_items=len(items), sums=sums,
+                             bins=bins, remaining=rem, t_done=tdone)
+            times = []
+            for rep in range(3):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                st = lib.pmo_run_batched(C.byref(b), C.byref(A.PmoLaunch(threads, 0)),
+                                         C.c_void_p(self.workspace.data_ptr()),
+                                         self.workspace.numel(), E._stream_handle())
+                e1.record()
+                check(st, "pmo_run_batched (autotune)")
+                torch.cuda.synchronize()
+                if rep:
+                    times.append(e0.elapsed_time(e1))
+            t = min(times)
+            if t < best_t:
+                best, best_t = (threads, chunk), t
+        _TUNE_CACHE[sig] = best
+        self.tune_table = {"best": best, "best_ms": best_t}
+        return best
+
+
+def time_batch(batch: SlabBatch, reps: int = 3) -> dict:
+    """Wall and device time of graph replays of the batch."""
+    if batch.graph is None:
+        batch.capture()
+    times = []
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        batch.graph.replay()
+        e1.record()
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1) / 1e3)
+    return {"seconds": min(times), "evals_per_s": batch.P / min(times)}
+
+
+def voxel_slab_problem(ma, ms, g, n, thickness, n_ambient=1.0, half: int = 60):
+    """One slab as the reference builds it with PlateModel: one z voxel of the
+    slab's thickness, 2*half+1 lateral voxels, end-label shell."""
+    from .problem import pencil_problem
+    k = 2 * half + 1
+    vol = np.ones((k + 2, k + 2, 3), np.uint8)
+    vol[1:-1, 1:-1, 1] = 0
+    return pencil_problem(vol, float(thickness), 1, [ma], [ms], [g], [n, n_ambient])
+
+
+def plain_eval(ma, ms, g, n, thickness, photons, *, nr=32, dr=0.1, seed=0, device=None) -> dict:
+    """One forward + gradient evaluation of one slab through the per-problem
+    API (upload, scored forward run, gradient replay): the path the batched
+    form replaces."""
+    from . import grad as G
+    prob = voxel_slab_problem(ma, ms, g, n, thickness)
+    dp = E.DeviceProblem(prob, device)
+    fwd = G.run_forward_scored(dp, int(photons), seed, nr, dr)
+    area = torch.tensor(G.annulus_area(nr, dr), dtype=torch.float64, device=dp.device)
+    coef = torch.zeros(A.PMO_RR_CATS, nr, dtype=torch.float32, device=dp.device)
+    coef[A.PMO_RR_TOP] = (1.0 / (area * photons)).float()
+    coef[A.PMO_RR_LAT_NEG] = coef[A.PMO_RR_TOP]
+    rep = G.run_replay(dp, fwd, coef, seed, per_voxel=False)
+    L = fwd.ledger.cpu().numpy()
+    return {"Rd": L[A.PMO_L_RD] / photons, "dR_dma": float(rep.d_ma_label[0]),
+            "dR_dms": float(rep.d_ms_label[0])}
+
+
+def batched_vs_plain(count: int = 4096, plain_sample: int = 48, seed: int = 0, nr: int = 32,
+                     dr: float = 0.1, device=None) -> dict:
+    """C5: ``count`` slabs with log-uniform budgets in one graph-captured
+    persistent launch (forward + gradient), against per-problem plain
+    evaluations of a random sample of the same problems."""
+    from . import volumes as V
+    b = V.c5_slab_batch(seed=seed, count=count)
+    t0 = time.perf_counter()
+    sb = SlabBatch(b["ma"], b["ms"], b["g"], b["n"], b["thickness"], b["n_photons"], nr=nr,
+                   dr=dr, seed=seed + 1, device=device)
+    tune_s = time.perf_counter() - t0
+    sb.capture()
+    tb = time_batch(sb, reps=2)
+    res = sb.fetch()
+    comp = res["completion_ms"]
+    rng = np.random.default_rng(seed + 7)
+    pick = rng.choice(count, size=min(plain_sample, count), replace=False)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in pick:
+        plain_eval(b["ma"][i], b["ms"][i], b["g"][i], b["n"][i], b["thickness"][i],
+                   int(b["n_photons"][i]), nr=nr, dr=dr, seed=seed + 1, device=device)
+    torch.cuda.synchronize()
+    plain_s = time.perf_counter() - t0
+    plain_rate = len(pick) / plain_s
+    # the same slab kernel launched once per problem (no batching, no graph)
+    singles = [SlabBatch([b["ma"][i]], [b["ms"][i]], [b["g"][i]], [b["n"][i]],
+                         [b["thickness"][i]], [int(b["n_photons"][i])], nr=nr, dr=dr,
+                         seed=seed + 1, device=device, autotune=False,
+                         block_threads=sb.block_threads, chunk=sb.chunk) for i in pick]
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for one in singles:
+        one.launch()
+        one.results.cpu()
+    torch.cuda.synchronize()
+    single_rate = len(pick) / (time.perf_counter() - t0)
+    photons = float(b["n_photons"].sum())
+    return {
+        "problems": count,
+        "photons": photons,
+        "batched_seconds": tb["seconds"],
+        "batched_evals_per_s": tb["evals_per_s"],
+        "batched_photons_per_s": photons / tb["seconds"],
+        "plain_evals_per_s": plain_rate,
+        "plain_sample": len(pick),
+        "ratio": tb["evals_per_s"] / plain_rate,
+        "single_launch_evals_per_s": single_rate,
+        "ratio_vs_single_launches": tb["evals_per_s"] / single_rate,
+        "p50_completion_ms": float(np.percentile(comp, 50)),
+        "p99_completion_ms": float(np.percentile(comp, 99)),
+        "launch_shape": {"block_threads": sb.block_threads, "photons_per_item": sb.chunk},
+        "autotune_seconds": tune_s,
+        "max_energy_residual": float(np.max(np.abs(res["balance"]))),
+    }

@@ -2,6 +2,7 @@
 // arithmetic type.  Included by vmc_plain_f32.cu and vmc_plain_f64.cu, which
 // are compiled with different floating-point flags.
 #pragma once
+#include "vmc_batched.cuh"
 #include "vmc_transport.cuh"
 
 namespace pmo {
@@ -89,6 +90,26 @@ cudaError_t launch_grad_r(const KParams &kp, int props, int threads, int bps, cu
     }
     return launch_plain_t<R, PMO_PROPS_VOXEL, PMO_FLU_NONE, false, true>(kp, threads, bps, s,
                                                                          nullptr);
+}
+
+template <typename R>
+cudaError_t launch_batched_r(const BParams &bp, int threads, int blocks_per_sm, cudaStream_t s) {
+    auto kern = vmc_batched_kernel<R>;
+    const size_t smem = (size_t)threads * kSlots * sizeof(double);
+    cudaError_t e;
+    if (smem > 48 * 1024) {
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    const int sms = device_sm_count();
+    if (sms <= 0) return cudaErrorNoDevice;
+    int occ = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, smem);
+    if (e != cudaSuccess) return e;
+    if (occ < 1) return cudaErrorInvalidConfiguration;
+    const int per_sm = blocks_per_sm > 0 && blocks_per_sm < occ ? blocks_per_sm : occ;
+    kern<<<sms * per_sm, threads, smem, s>>>(bp);
+    return cudaGetLastError();
 }
 
 }  // namespace pmo

@@ -12,4 +12,7 @@ cudaError_t launch_grad_f32(const KParams &kp, int props, int threads, int bps,
                             cudaStream_t s) {
     return launch_grad_r<float>(kp, props, threads, bps, s);
 }
+cudaError_t launch_batched_f32(const BParams &bp, int threads, int bps, cudaStream_t s) {
+    return launch_batched_r<float>(bp, threads, bps, s);
+}
 }  // namespace pmo

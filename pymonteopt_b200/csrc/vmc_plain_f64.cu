@@ -13,4 +13,7 @@ cudaError_t launch_grad_f64(const KParams &kp, int props, int threads, int bps,
                             cudaStream_t s) {
     return launch_grad_r<double>(kp, props, threads, bps, s);
 }
+cudaError_t launch_batched_f64(const BParams &bp, int threads, int bps, cudaStream_t s) {
+    return launch_batched_r<double>(bp, threads, bps, s);
+}
 }  // namespace pmo
