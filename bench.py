@@ -50,6 +50,8 @@ def parse_args():
     ap.add_argument("--photons", type=float, default=1e8, help="photons per step per GPU")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched+gradient vs plain comparison (4096 slabs)")
     ap.add_argument("--block-threads", type=int, default=0)
     ap.add_argument("--blocks-per-sm", type=int, default=0)
     return ap.parse_args()
@@ -66,7 +68,7 @@ def config_dict(photons: int, world: int) -> dict:
         "photons_per_step_per_gpu": photons,
         "rr_bins": [100, 0.1],
         "fluence_tally": False,
-        "l2": "flushed between timed steps (256 MiB write); label volume 65 MB < L2",
+        "l2": "flushed between timed steps (256 MiB write); uint16 voxel-word map 130 MB",
         "parallelism": f"replicas x{world} (photon ranges per GPU, no collectives)",
     }
 
@@ -364,6 +366,13 @@ def main() -> int:
         e2e = {"value": total_photons / float(e_s.item()), "unit": UNIT,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
 
+    batched = None
+    if rank == 0 and world == 1 and not args.no_batched:
+        # second half of the metric: 4096 slab problems, forward + gradient in
+        # one graph-captured persistent launch vs per-problem plain evaluations
+        from pymonteopt_b200 import batched as B
+        batched = B.batched_vs_plain(count=4096, device=dev)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = cpu_oracle_rate(12.0)
@@ -387,6 +396,7 @@ def main() -> int:
         "cpu_baseline": cpu,
         "e2e": e2e,
         "gpu_launches": args.steps,
+        "batched": batched,
         "clocks": clk,
         "wall_s_timed_region": wall,
         "results": results,
