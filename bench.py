@@ -52,6 +52,9 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched+gradient vs plain comparison (4096 slabs)")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference's own cuVMC kernel on the 256^3 volume")
+    ap.add_argument("--ref-gpu-photons", type=float, default=1e7)
     ap.add_argument("--block-threads", type=int, default=0)
     ap.add_argument("--blocks-per-sm", type=int, default=0)
     return ap.parse_args()
@@ -189,6 +192,108 @@ def run_reference(args, rank: int, world: int) -> None:
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def reference_gpu_leg(torch, dev, photons: int) -> dict:
+    """The reference's own GPU kernel cuVMC (pymopt/voxel_gpu/_cukernel.py,
+    compiled unchanged into oracle/_ref) against this kernel on the 256^3
+    CT-like volume with a pencil beam, the same photon count on each side.
+
+    * kernel: state (reference) or volume (ours) resident on the device,
+      CUDA events around the launch;
+    * e2e: the reference's start() traffic, i.e. 40 B/photon of state copied
+      from pinned host memory and back; ours copies the label volume in and
+      the tallies out.
+    """
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import ref_gpu  # noqa: E402  (reference kernel: baseline only)
+    from pymonteopt_b200 import _abi as A
+    from pymonteopt_b200 import engine as E
+    from pymonteopt_b200 import volumes as V
+    if not ref_gpu.available():
+        return {"unavailable": "oracle/_ref/libcuvmc_ref.so was not built (reference tree absent)"}
+    prob = V.c3_ct_like(0)
+    stream = torch.cuda.current_stream()
+
+    def timed(fn, reps=3):
+        best = float("inf")
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            a.record(stream)
+            fn()
+            b.record(stream)
+            torch.cuda.synchronize()
+            best = min(best, a.elapsed_time(b) / 1e3)
+        return best
+
+    ref = ref_gpu.RefVolume(prob, dev)
+    warm = ref.initial_state(100000)
+    ref.launch(*warm, seed=1)
+    state = ref.initial_state(photons)
+    fresh = [t.clone() for t in state]
+
+    def ref_kernel():
+        for d, s0 in zip(state, fresh):
+            d.copy_(s0)
+        ref.launch(*state, seed=7)
+    # the state reset is a device copy of 40 B/photon, timed apart and removed
+    t_reset = timed(lambda: [d.copy_(s0) for d, s0 in zip(state, fresh)])
+    t_ref = max(timed(ref_kernel) - t_reset, 1e-9)
+    ref_res = ref.results(*state, nr=100, dr=0.2)
+
+    host = [t.cpu().pin_memory() for t in fresh]
+    back = [torch.empty_like(h).pin_memory() for h in host]
+
+    def ref_e2e():
+        for d, h in zip(state, host):
+            d.copy_(h, non_blocking=True)
+        ref.launch(*state, seed=8)
+        for h, d in zip(back, state):
+            h.copy_(d, non_blocking=True)
+    t_ref_e2e = timed(ref_e2e)
+
+    out = {"workload": "c3_ct_like_256^3_pencil", "photons": photons,
+           "reference": {"kernel_photons_per_s": photons / t_ref,
+                         "e2e_photons_per_s": photons / t_ref_e2e,
+                         "Rd": ref_res["Rd"], "Tt": ref_res["Tt"],
+                         "source": "pymopt/voxel_gpu/_cukernel.py cuVMC, nvcc sm_100a, "
+                                   "128 threads/block, one thread per photon"}}
+    dp = E.DeviceProblem(prob, dev)
+    pinned_labels = torch.from_numpy(prob.labels).pin_memory()
+    for name, flu in (("ours", A.PMO_FLU_NONE), ("ours_with_fluence", A.PMO_FLU_GLOBAL)):
+        spec = E.TallySpec(nr=100, dr=0.2, fluence=flu)
+        t = E.run_plain(dp, 100000, 1, spec=spec)
+        tal = E.Tallies(dp, spec, photons)
+
+        def ours_kernel():
+            tal.zero_()
+            E.run_plain(dp, photons, 7, tallies=tal)
+        t_zero = timed(tal.zero_)
+        t_ours = max(timed(ours_kernel) - t_zero, 1e-9)
+        tal.check()
+        led = tal.ledger.cpu().numpy()
+        host_led = torch.empty_like(tal.ledger, device="cpu").pin_memory()
+        host_rr = torch.empty_like(tal.rr, device="cpu").pin_memory()
+        host_abs = (torch.empty_like(tal.absorbed, device="cpu").pin_memory()
+                    if tal.absorbed is not None else None)
+
+        def ours_e2e():
+            dp.labels.copy_(pinned_labels, non_blocking=True)
+            tal.zero_()
+            E.run_plain(dp, photons, 8, tallies=tal)
+            host_led.copy_(tal.ledger, non_blocking=True)
+            host_rr.copy_(tal.rr, non_blocking=True)
+            if host_abs is not None:
+                host_abs.copy_(tal.absorbed, non_blocking=True)
+        t_ours_e2e = timed(ours_e2e)
+        out[name] = {"kernel_photons_per_s": photons / t_ours,
+                     "e2e_photons_per_s": photons / t_ours_e2e,
+                     "Rd": float(led[A.PMO_L_RD] / photons),
+                     "Tt": float(led[A.PMO_L_TT] / photons)}
+    out["speedup_kernel"] = out["ours"]["kernel_photons_per_s"] / out["reference"]["kernel_photons_per_s"]
+    out["speedup_e2e"] = out["ours"]["e2e_photons_per_s"] / out["reference"]["e2e_photons_per_s"]
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -373,6 +478,10 @@ def main() -> int:
         from pymonteopt_b200 import batched as B
         batched = B.batched_vs_plain(count=4096, device=dev)
 
+    reference_gpu = None
+    if rank == 0 and world == 1 and not args.no_reference_gpu:
+        reference_gpu = reference_gpu_leg(torch, dev, int(args.ref_gpu_photons))
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = cpu_oracle_rate(12.0)
@@ -397,6 +506,7 @@ def main() -> int:
         "e2e": e2e,
         "gpu_launches": args.steps,
         "batched": batched,
+        "reference_gpu": reference_gpu,
         "clocks": clk,
         "wall_s_timed_region": wall,
         "results": results,

@@ -152,3 +152,24 @@ def test_model_builds_transport_problem():
     prob.validate()
     assert prob.source == A.PMO_SRC_GAUSSIAN and prob.beam_sigma == 0.5
     assert prob.end_label == 2 and prob.n_labels == 3
+
+
+def test_reference_kernel_library_builds_and_exports():
+    """oracle/ref_gpu_build.py: the reference's cuVMC source string is found
+    and compiled; the launcher is exported (no GPU call)."""
+    import ctypes
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(GOLDEN), "..", "oracle"))
+    try:
+        import ref_gpu_build
+    finally:
+        sys.path.pop(0)
+    kernel_py = os.path.join(ref_gpu_build.REFERENCE_ROOT, ref_gpu_build.KERNEL_PY)
+    if os.path.exists(kernel_py):
+        src = ref_gpu_build.extract()
+        assert "__global__ void cuVMC(" in src and "curand_init" in src
+        ref_gpu_build.build()
+    if not ref_gpu_build.available():
+        pytest.skip("reference tree absent and no prebuilt reference kernel")
+    lib = ctypes.CDLL(ref_gpu_build.LIB)
+    assert hasattr(lib, "ref_cuvmc_launch")
