@@ -10,6 +10,34 @@
 
 namespace pmo {
 
+// The ten round keys (k0 + r*W0, k1 + r*W1), r = 0..9, of one key.  Kernels
+// get them precomputed in their launch parameters, so each round's key is a
+// constant-bank operand instead of two adds per round.
+struct PhiloxKeys {
+    uint32_t k[20];
+};
+
+__host__ __device__ inline PhiloxKeys philox_round_keys(uint32_t k0, uint32_t k1) {
+    PhiloxKeys rk;
+    for (int r = 0; r < 10; ++r) {
+        rk.k[2 * r] = k0 + (uint32_t)r * 0x9E3779B9u;
+        rk.k[2 * r + 1] = k1 + (uint32_t)r * 0xBB67AE85u;
+    }
+    return rk;
+}
+
+__device__ __forceinline__ uint4 philox4x32_10(uint4 c, const PhiloxKeys &rk) {
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        const uint32_t lo0 = 0xD2511F53u * c.x;
+        const uint32_t hi0 = __umulhi(0xD2511F53u, c.x);
+        const uint32_t lo1 = 0xCD9E8D57u * c.z;
+        const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z);
+        c = make_uint4(hi1 ^ c.y ^ rk.k[2 * r], lo1, hi0 ^ c.w ^ rk.k[2 * r + 1], lo0);
+    }
+    return c;
+}
+
 __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
 #pragma unroll
     for (int r = 0; r < 10; ++r) {

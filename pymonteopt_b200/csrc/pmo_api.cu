@@ -126,6 +126,7 @@ int problem_to_params(const pmo_problem *p, KParams *kp) {
     kp->state_w = p->state_w;
     kp->key0 = (uint32_t)p->seed;
     kp->key1 = (uint32_t)(p->seed >> 32);
+    kp->rk = pmo::philox_round_keys(kp->key0, kp->key1);
     kp->begin = p->photon_begin;
     kp->count = p->photon_count;
     kp->max_events = p->max_events;

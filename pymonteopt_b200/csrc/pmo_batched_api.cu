@@ -83,6 +83,7 @@ int pmo_run_batched(const pmo_batch *b, const pmo_launch *launch, void *workspac
     bp.n_items = b->n_items;
     bp.key0 = (uint32_t)b->seed;
     bp.key1 = (uint32_t)(b->seed >> 32);
+    bp.rk = pmo::philox_round_keys(bp.key0, bp.key1);
     bp.nr = b->nr;
     bp.sums = b->sums;
     bp.bins = b->bins;

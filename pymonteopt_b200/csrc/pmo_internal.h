@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/pmo_b200.h"
+#include "philox.cuh"
 
 namespace pmo {
 
@@ -32,6 +33,7 @@ struct KParams {
     float *state_p, *state_v, *state_w;
     // photons
     uint32_t key0, key1;
+    PhiloxKeys rk;                 // round keys of (key0, key1)
     uint64_t begin, count;
     uint32_t max_events;
     uint32_t flags;

@@ -29,6 +29,7 @@ struct BParams {
     const pmo_batch_item *items;
     int32_t n_items;
     uint32_t key0, key1;
+    PhiloxKeys rk;                 // round keys of (key0, key1)
     int32_t nr;
     double *sums;
     float *bins;
@@ -59,7 +60,6 @@ __global__ void __launch_bounds__(512) vmc_batched_kernel(const BParams bp) {
 
     const unsigned FULL = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31u;
-    const uint2 key = make_uint2(bp.key0, bp.key1);
     const uint32_t cap = bp.max_events ? bp.max_events : (1u << 26);
 
     int acc_p = -1;  // problem held in acc[]
@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(512) vmc_batched_kernel(const BParams bp) {
 
     // one interaction cycle; returns true while the photon is in flight
     auto cycle = [&]() -> bool {
-        const uint4 rn = philox4x32_10(make_uint4(k, 4u * (uint32_t)p, j, 0u), key);
+        const uint4 rn = philox4x32_10(make_uint4(k, 4u * (uint32_t)p, j, 0u), bp.rk);
         ++k;
         R st = pneglog(u01<R>(rn.x));
         for (;;) {
@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(512) vmc_batched_kernel(const BParams bp) {
             bool transmit = true;
             R cb = R(1), nr = R(1);
             if (nin != nout) {
-                const uint4 fr = philox4x32_10(make_uint4(f, 1u + 4u * (uint32_t)p, j, 0u), key);
+                const uint4 fr = philox4x32_10(make_uint4(f, 1u + 4u * (uint32_t)p, j, 0u), bp.rk);
                 ++f;
                 const R u = u01<R>(fr.x);
                 R ca = fabs(vz);

@@ -190,7 +190,6 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
 
     const unsigned FULL = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31u;
-    const uint2 key = make_uint2(kp.key0, kp.key1);
     const R l = (R)kp.l;
     const R hl = (R)kp.hl;
     const R inv_l = (R)kp.inv_l;
@@ -456,7 +455,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             vz = (R)kp.src_v[2];
             w = (R)kp.src_w0;
             if (kp.source == PMO_SRC_GAUSSIAN || kp.spec_prob > 0.f) {
-                const uint4 rs = philox4x32_10(make_uint4(0u, 2u, (uint32_t)pid, (uint32_t)(pid >> 32)), key);
+                const uint4 rs = philox4x32_10(make_uint4(0u, 2u, (uint32_t)pid, (uint32_t)(pid >> 32)), kp.rk);
                 if (kp.source == PMO_SRC_GAUSSIAN) {
                     // x, y ~ N(0, sigma) (gaussianBeam, :267-287) by Box-Muller,
                     // split into voxel index + offset in [-l/2, l/2] (:242-252)
@@ -521,7 +520,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
     auto cycle = [&]() -> bool {
         if (!pending) {
             const uint4 rn =
-                philox4x32_10(make_uint4(k, 0u, (uint32_t)pid, (uint32_t)(pid >> 32)), key);
+                philox4x32_10(make_uint4(k, 0u, (uint32_t)pid, (uint32_t)(pid >> 32)), kp.rk);
             ++k;
             st = pneglog(u01<R>(rn.x));  // step in optical depths (:75)
             ry = rn.y;
@@ -626,7 +625,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             if (ni != nt) {
                 // Fresnel / total internal reflection (:105-153) with the
                 // cosines and sines of the incidence/transmission angles
-                const uint4 fr = philox4x32_10(make_uint4(f, 1u, (uint32_t)pid, (uint32_t)(pid >> 32)), key);
+                const uint4 fr = philox4x32_10(make_uint4(f, 1u, (uint32_t)pid, (uint32_t)(pid >> 32)), kp.rk);
                 ++f;
                 const R u = u01<R>(fr.x);
                 R ca = fabs(va);
