@@ -62,6 +62,7 @@ extern "C" {
 /* ---- fluence tally modes ------------------------------------------------ */
 #define PMO_FLU_NONE     0
 #define PMO_FLU_GLOBAL   1       /* fp32 atomics straight to the padded grid    */
+#define PMO_ABSORBED_SHIFT 32   /* fixed-point scale of the absorbed grid */
 #define PMO_FLU_SHARED   2       /* + per-block shared-memory window            */
 
 /* ---- ledger slots (double), accumulated by the kernels ------------------ */
@@ -156,7 +157,11 @@ typedef struct pmo_tallies {
     int32_t nr;
     float dr;                         /* bin width [mm]; bins (i*dr, (i+1)*dr] */
     int32_t fluence_mode;             /* PMO_FLU_* */
-    float *absorbed;                  /* nx*ny*nz absorbed weight, accumulated */
+    /* nx*ny*nz absorbed weight, accumulated, in unsigned 64-bit fixed point:
+       weight * 2^PMO_ABSORBED_SHIFT per deposit, rounded to nearest.
+       Integer atomics make each voxel's sum exact and independent of the
+       order of the deposits. */
+    unsigned long long *absorbed;
     int32_t win_lo[3];                /* PMO_FLU_SHARED: window origin (voxel) */
     int32_t win_dim[3];               /* PMO_FLU_SHARED: window extent (voxels) */
     /* PMO_FLAG_EXPORT_EXITS: final state per photon (index photon - begin).
@@ -369,13 +374,14 @@ int pmo_cuvmc(int32_t *add, float *p, float *v, float *w,
               void *workspace, size_t workspace_bytes, void *stream);
 
 /*
- * Fluence normalisation in FP64: phi = absorbed / (n_photons * l^3 * mu_a)
+ * Fluence normalisation in FP64: phi = absorbed * 2^-PMO_ABSORBED_SHIFT
+ * / (n_photons * l^3 * mu_a)
  * over the interior (nx-2, ny-2, nz-2) of the padded grid; voxels with
  * mu_a == 0 get 0.  mu_a comes from the label table or the voxel grid of
  * `prob`.  No counterpart in the reference GPU path (the reference tallies
  * fluence only in pymopt/fluence/intarnal_fluence.py:12-152, on the host).
  */
-int pmo_normalize_fluence(const pmo_problem *prob, const float *absorbed,
+int pmo_normalize_fluence(const pmo_problem *prob, const unsigned long long *absorbed,
                           double n_photons, double *phi_out, void *stream);
 
 /* Philox4x32-10 words of the engine's generator for n counters ctr[4*n]

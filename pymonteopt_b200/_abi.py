@@ -33,6 +33,7 @@ PMO_PROPS_VOXEL = 1
 PMO_FLU_NONE = 0
 PMO_FLU_GLOBAL = 1
 PMO_FLU_SHARED = 2
+PMO_ABSORBED_SHIFT = 32
 
 PMO_L_WINIT = 0
 PMO_L_RD = 1

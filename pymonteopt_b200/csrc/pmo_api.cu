@@ -14,8 +14,9 @@ cudaError_t launch_plain_f64(const KParams &kp, int props, int flu, int threads,
 cudaError_t launch_grad_f32(const KParams &kp, int props, int threads, int bps, cudaStream_t s);
 cudaError_t launch_grad_f64(const KParams &kp, int props, int threads, int bps, cudaStream_t s);
 
-// phi = absorbed / (n_photons * l^3 * mu_a) over the interior voxels, FP64.
-__global__ void normalize_fluence_kernel(const float *__restrict__ absorbed,
+// phi = absorbed * 2^-PMO_ABSORBED_SHIFT / (n_photons * l^3 * mu_a) over the
+// interior voxels, FP64.
+__global__ void normalize_fluence_kernel(const unsigned long long *__restrict__ absorbed,
                                          const uint8_t *__restrict__ labels,
                                          const float *__restrict__ ma_tab,
                                          const float *__restrict__ vox_ma, int props_mode,
@@ -34,10 +35,11 @@ __global__ void normalize_fluence_kernel(const float *__restrict__ absorbed,
     }
 }
 
-cudaError_t launch_normalize_fluence(const KParams &kp, int props_mode, const float *absorbed,
+cudaError_t launch_normalize_fluence(const KParams &kp, int props_mode,
+                                     const unsigned long long *absorbed,
                                      double n_photons, double *phi, cudaStream_t stream) {
     const double l = (double)kp.l;
-    const double scale = 1.0 / (n_photons * l * l * l);
+    const double scale = 1.0 / (n_photons * l * l * l) / (double)(1ull << PMO_ABSORBED_SHIFT);
     const uint64_t total = (uint64_t)(kp.nx - 2) * (kp.ny - 2) * (kp.nz - 2);
     uint64_t blocks = (total + 255) / 256;
     if (blocks > 148 * 32) blocks = 148 * 32;
@@ -150,7 +152,7 @@ int tallies_to_params(const pmo_problem *p, const pmo_tallies *t, KParams *kp) {
                 return PMO_ERR_ARG;
             cells *= (uint64_t)t->win_dim[a];
         }
-        if (cells * sizeof(float) > 160 * 1024) return PMO_ERR_ARG;
+        if (cells * sizeof(unsigned long long) > 160 * 1024) return PMO_ERR_ARG;
     }
     if ((p->flags & PMO_FLAG_EXPORT_EXITS) &&
         (!t->exit_add || !t->exit_p || !t->exit_v || !t->exit_w))
@@ -343,7 +345,8 @@ int pmo_cuvmc(int32_t *add, float *p, float *v, float *w, const float *ma, const
     return launch_kp(kp, PMO_FP32, PMO_PROPS_LABEL, PMO_FLU_NONE, nullptr, s);
 }
 
-int pmo_normalize_fluence(const pmo_problem *prob, const float *absorbed, double n_photons,
+int pmo_normalize_fluence(const pmo_problem *prob, const unsigned long long *absorbed,
+                          double n_photons,
                           double *phi_out, void *stream) {
     KParams kp;
     int st = problem_to_params(prob, &kp);

@@ -44,7 +44,7 @@ struct KParams {
     int32_t nr;
     float dr;
     int32_t rr_shared;             // histogram privatised in shared memory
-    float *absorbed;
+    unsigned long long *absorbed;  // fixed point, 2^PMO_ABSORBED_SHIFT per unit
     int32_t win_lo[3], win_dim[3]; // shared fluence window (PMO_FLU_SHARED)
     int32_t *exit_add;
     float *exit_p, *exit_v, *exit_w;
@@ -77,7 +77,8 @@ cudaError_t launch_grad(const KParams &kp, int precision, int props_mode, int bl
 cudaError_t launch_plain(const KParams &kp, int precision, int props_mode, int fluence_mode,
                          int block_threads, int blocks_per_sm, cudaStream_t stream,
                          LaunchShape *shape_out);
-cudaError_t launch_normalize_fluence(const KParams &kp, int props_mode, const float *absorbed,
+cudaError_t launch_normalize_fluence(const KParams &kp, int props_mode,
+                                     const unsigned long long *absorbed,
                                      double n_photons, double *phi, cudaStream_t stream);
 
 size_t plain_smem_bytes(int precision, int nr, int rr_shared, int fluence_mode,

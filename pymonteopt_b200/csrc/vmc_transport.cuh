@@ -13,8 +13,9 @@
 // Per block: the per-label property table (mt, 1/mt, ma/mt, n and the
 // Henyey-Greenstein constants) lives in shared memory; R(r)/T(r) histograms and
 // the FP64 ledger are privatised in shared memory and flushed once at the end;
-// the absorbed-weight grid gets fp32 atomics, merged in registers while a
-// photon stays in one voxel and optionally privatised in a shared window.
+// the absorbed-weight grid gets 64-bit fixed-point integer atomics (exact and
+// order-independent), merged in registers while a photon stays in one voxel
+// and optionally privatised in a shared window.
 #pragma once
 #include <cstdint>
 
@@ -92,6 +93,15 @@ __device__ __forceinline__ void make_props(LabelProps<R> &t, float ma, float ms,
     t.pad1 = t.pad2 = R(0);
 }
 
+// Weight -> fixed point of the absorbed grid, rounded to nearest.  dw <= 1,
+// so one deposit is at most 2^PMO_ABSORBED_SHIFT.
+__device__ __forceinline__ unsigned long long to_fixed(float dw) {
+    return __float2ull_rn(__fmul_rn(dw, (float)(1ull << PMO_ABSORBED_SHIFT)));
+}
+__device__ __forceinline__ unsigned long long to_fixed(double dw) {
+    return __double2ull_rn(dw * (double)(1ull << PMO_ABSORBED_SHIFT));
+}
+
 // theta(g, rand) of the reference (pymopt/voxel_gpu/_cukernel.py:14-25)
 template <typename R>
 __device__ __forceinline__ R hg_cos(const LabelProps<R> &t, R u) {
@@ -118,7 +128,8 @@ struct SmemLayout {
     }
     __host__ __device__ static size_t total(int nr, int rr_shared, int flu, const int32_t win_dim[3]) {
         size_t o = win_off(nr, rr_shared);
-        if (flu == PMO_FLU_SHARED) o += (size_t)win_dim[0] * win_dim[1] * win_dim[2] * sizeof(float);
+        if (flu == PMO_FLU_SHARED)
+            o += (size_t)win_dim[0] * win_dim[1] * win_dim[2] * sizeof(unsigned long long);
         return (o + 15) & ~size_t(15);
     }
     // gradient replay with the reweighted finite difference: per-target sums
@@ -157,7 +168,8 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
     R *s_rr = reinterpret_cast<R *>(smem_raw + L::rr_off);
     double *s_gma = reinterpret_cast<double *>(smem_raw + L::gl_off);
     double *s_gms = s_gma + 256;
-    float *s_win = reinterpret_cast<float *>(smem_raw + L::win_off(kp.nr, kp.rr_shared));
+    unsigned long long *s_win =
+        reinterpret_cast<unsigned long long *>(smem_raw + L::win_off(kp.nr, kp.rr_shared));
     const int n_win = FLU == PMO_FLU_SHARED ? kp.win_dim[0] * kp.win_dim[1] * kp.win_dim[2] : 0;
     const bool fd = GRAD && kp.fd_n > 0;
     double *s_fdsum = reinterpret_cast<double *>(
@@ -185,7 +197,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
     for (int i = threadIdx.x; i < PMO_COUNTERS_N; i += blockDim.x) s_cnt[i] = 0ull;
     if (kp.rr_shared)
         for (int i = threadIdx.x; i < PMO_RR_CATS * kp.nr; i += blockDim.x) s_rr[i] = R(0);
-    for (int i = threadIdx.x; i < n_win; i += blockDim.x) s_win[i] = 0.f;
+    for (int i = threadIdx.x; i < n_win; i += blockDim.x) s_win[i] = 0ull;
     __syncthreads();
 
     const unsigned FULL = 0xffffffffu;
@@ -223,11 +235,11 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
     float gq = 0.f, gL = 0.f, gN = 0.f, gC = 0.f;
     R ims = 0;
     uint32_t pend_lin = 0xffffffffu;
-    float pend_w = 0.f;
+    unsigned long long pend_q = 0;   // fixed-point deposit not yet written
 
     auto deposit_flush = [&]() {
-        if (pend_w != 0.f) atomicAdd(kp.absorbed + pend_lin, pend_w);
-        pend_w = 0.f;
+        if (pend_q != 0ull) atomicAdd(kp.absorbed + pend_lin, pend_q);
+        pend_q = 0ull;
         pend_lin = 0xffffffffu;
     };
     // offset of the voxel holding the photon from the box centre, in voxels
@@ -236,7 +248,8 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
         int k = (int)rint(xmul(q, inv_l));
         return k < -m ? -m : (k > m ? m : k);
     };
-    auto deposit = [&](float dw) {
+    auto deposit = [&](R dw) {
+        const unsigned long long q = to_fixed(dw);
         int cx = ix, cy = iy, cz = iz;
         uint32_t clin = lin;
         if (SKIP && rad > 1) {
@@ -258,16 +271,16 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             const unsigned wz = (unsigned)(cz - kp.win_lo[2]);
             if (wx < (unsigned)kp.win_dim[0] && wy < (unsigned)kp.win_dim[1] &&
                 wz < (unsigned)kp.win_dim[2]) {
-                atomicAdd(s_win + ((wx * kp.win_dim[1] + wy) * kp.win_dim[2] + wz), dw);
+                atomicAdd(s_win + ((wx * kp.win_dim[1] + wy) * kp.win_dim[2] + wz), q);
                 return;
             }
         }
         if (clin == pend_lin) {
-            pend_w += dw;
+            pend_q += q;
         } else {
             deposit_flush();
             pend_lin = clin;
-            pend_w = dw;
+            pend_q = q;
         }
     };
     auto set_dir_inverse = [&]() {
@@ -694,7 +707,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             const double dw = (double)w - (double)wn;
             w = wn;
             t_abs += dw;
-            if (FLU != PMO_FLU_NONE) deposit((float)dw);
+            if (FLU != PMO_FLU_NONE) deposit((R)dw);
         }
         // Russian roulette (:182-195)
         if (w <= R(0.0001)) {
@@ -803,7 +816,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
     if (FLU == PMO_FLU_SHARED) {
         const int wy = kp.win_dim[1], wz = kp.win_dim[2];
         for (int i = threadIdx.x; i < n_win; i += blockDim.x) {
-            if (s_win[i] != 0.f) {
+            if (s_win[i] != 0ull) {
                 const int a = i / (wy * wz), b = (i / wz) % wy, c = i % wz;
                 const uint32_t g = ((uint32_t)(kp.win_lo[0] + a) * (uint32_t)kp.ny +
                                     (uint32_t)(kp.win_lo[1] + b)) * (uint32_t)kp.nz +

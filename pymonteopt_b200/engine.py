@@ -133,7 +133,9 @@ class Tallies:
         self.counters = torch.zeros(A.PMO_COUNTERS_N, dtype=torch.int64, device=dev)
         self.rr = (torch.zeros(A.PMO_RR_CATS, spec.nr, dtype=torch.float32, device=dev)
                    if spec.nr > 0 else None)
-        self.absorbed = (torch.zeros(dprob.labels.shape, dtype=torch.float32, device=dev)
+        # absorbed weight per voxel in 64-bit fixed point (2^PMO_ABSORBED_SHIFT
+        # per unit weight; int64 storage of the kernel's unsigned sums)
+        self.absorbed = (torch.zeros(dprob.labels.shape, dtype=torch.int64, device=dev)
                          if spec.fluence != A.PMO_FLU_NONE else None)
         N = self.capacity
         if spec.export_exits:
@@ -226,6 +228,13 @@ def run_plain(dprob: DeviceProblem, n_photons: int, seed: int, *, tallies: Talli
     check(st, "pmo_run_plain")
     tallies.n_photons += int(n_photons)
     return tallies
+
+
+def absorbed_weight(tallies: Tallies) -> torch.Tensor:
+    """The absorbed-weight grid as FP64 weight (fixed point / 2^32)."""
+    if tallies.absorbed is None:
+        raise ValueError("the run did not tally fluence")
+    return tallies.absorbed.double() * (2.0 ** -A.PMO_ABSORBED_SHIFT)
 
 
 def normalize_fluence(dprob: DeviceProblem, tallies: Tallies, stream=None) -> torch.Tensor:

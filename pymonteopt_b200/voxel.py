@@ -708,7 +708,8 @@ class BaseVoxelMonteCarlo(metaclass=ABCMeta):
 
     def get_absorbed(self):
         """Absorbed weight per voxel of the padded grid, divided by nPh."""
-        return self._tallies.absorbed.cpu().numpy().astype(np.float64) / self.nPh
+        from . import engine as E
+        return E.absorbed_weight(self._tallies).cpu().numpy() / self.nPh
 
     # ---- persistence (pymopt/voxel_gpu/_classes.py:338-382) -----------------
     def save_result(self, fname, *, coment="", save_monte=True, save_params=True):
