@@ -175,6 +175,21 @@ typedef struct pmo_tallies {
        to (category * nr + bin, -1 for none) and that weight */
     int32_t *score_bin;
     float *score_w;
+    /* Angle-resolved exits (pymopt/metrics/_scoring.py:27-38): weight per bin
+       (i*da, (i+1)*da] of arccos|v_z|, da = pi / (2 * n_ang); row 0 holds
+       exits with v_z < 0, row 1 those with v_z > 0.  2 * n_ang floats,
+       accumulated; n_ang = 0 or ang = NULL: off. */
+    float *ang;
+    int32_t n_ang;
+    /* Line profile of exits moving towards -x (the side-face profile of
+       pymopt/virtualOBD.py:171-172 through pymopt/metrics/_scoring.py:40-51):
+       weight per bin (i*line_dr, (i+1)*line_dr] of the exit depth
+       z = l*(add_z - 1) + p_z + l/2 (rounded to 1e-6 mm) for |y| < line_y_range.
+       n_line floats, accumulated; n_line = 0 or line = NULL: off. */
+    float *line;
+    int32_t n_line;
+    float line_dr;
+    float line_y_range;
 } pmo_tallies;
 
 /*

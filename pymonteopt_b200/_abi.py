@@ -143,6 +143,12 @@ class PmoTallies(C.Structure):
         ("exit_v", C.c_void_p), ("exit_w", C.c_void_p),
         ("ph_interact", C.c_void_p), ("ph_cross", C.c_void_p), ("ph_fresnel", C.c_void_p),
         ("score_bin", C.c_void_p), ("score_w", C.c_void_p),
+        ("ang", C.c_void_p),
+        ("n_ang", C.c_int32),
+        ("line", C.c_void_p),
+        ("n_line", C.c_int32),
+        ("line_dr", C.c_float),
+        ("line_y_range", C.c_float),
     ]
 
 

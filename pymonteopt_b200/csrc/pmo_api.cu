@@ -140,6 +140,10 @@ int tallies_to_params(const pmo_problem *p, const pmo_tallies *t, KParams *kp) {
     if (!t || !t->ledger || !t->counters) return PMO_ERR_ARG;
     if (t->nr < 0) return PMO_ERR_ARG;
     if (t->nr > 0 && (!t->rr || !finite_pos(t->dr))) return PMO_ERR_ARG;
+    if (t->ang && (t->n_ang < 0 || t->n_ang > 1 << 20)) return PMO_ERR_ARG;
+    if (t->line && (t->n_line < 0 || t->n_line > 1 << 20 ||
+                    (t->n_line > 0 && (!finite_pos(t->line_dr) || !finite_pos(t->line_y_range)))))
+        return PMO_ERR_ARG;
     if (t->fluence_mode != PMO_FLU_NONE && t->fluence_mode != PMO_FLU_GLOBAL &&
         t->fluence_mode != PMO_FLU_SHARED)
         return PMO_ERR_ARG;
@@ -164,8 +168,17 @@ int tallies_to_params(const pmo_problem *p, const pmo_tallies *t, KParams *kp) {
     kp->rr = t->rr;
     kp->nr = t->nr;
     kp->dr = t->dr;
-    // privatise the histogram in shared memory when it is small
-    kp->rr_shared = (t->nr > 0 && t->nr <= 1024) ? 1 : 0;
+    kp->n_ang = t->ang ? t->n_ang : 0;
+    kp->ang = t->ang;
+    kp->inv_da = kp->n_ang > 0 ? (float)(2.0 * kp->n_ang / 3.14159265358979323846) : 0.f;
+    kp->n_line = t->line ? t->n_line : 0;
+    kp->line = t->line;
+    kp->line_dr = t->line_dr;
+    kp->line_y = t->line_y_range;
+    // privatise the exit histograms in shared memory when they are small
+    const int hist = PMO_RR_CATS * (t->nr > 0 ? t->nr : 0) + 2 * kp->n_ang + kp->n_line;
+    kp->rr_shared = (hist > 0 && hist <= 4096) ? 1 : 0;
+    kp->hist_n = kp->rr_shared ? hist : 0;
     kp->absorbed = t->absorbed;
     for (int a = 0; a < 3; ++a) {
         kp->win_lo[a] = t->win_lo[a];

@@ -43,7 +43,17 @@ struct KParams {
     float *rr;
     int32_t nr;
     float dr;
-    int32_t rr_shared;             // histogram privatised in shared memory
+    // exit histograms: angle-resolved (2 x n_ang) and line profile (n_line)
+    float *ang;
+    int32_t n_ang;
+    float inv_da;                  // 2 * n_ang / pi
+    float *line;
+    int32_t n_line;
+    float line_dr, line_y;
+    // R(r), angle and line histograms privatised in shared memory (hist_n
+    // entries: PMO_RR_CATS * nr + 2 * n_ang + n_line) when they are small
+    int32_t rr_shared;
+    int32_t hist_n;
     unsigned long long *absorbed;  // fixed point, 2^PMO_ABSORBED_SHIFT per unit
     int32_t win_lo[3], win_dim[3]; // shared fluence window (PMO_FLU_SHARED)
     int32_t *exit_add;
@@ -80,8 +90,5 @@ cudaError_t launch_plain(const KParams &kp, int precision, int props_mode, int f
 cudaError_t launch_normalize_fluence(const KParams &kp, int props_mode,
                                      const unsigned long long *absorbed,
                                      double n_photons, double *phi, cudaStream_t stream);
-
-size_t plain_smem_bytes(int precision, int nr, int rr_shared, int fluence_mode,
-                        const int32_t win_dim[3]);
 
 }  // namespace pmo

@@ -25,7 +25,7 @@ template <typename R, int PROPS, int FLU, bool SKIP, bool GRAD = false>
 cudaError_t launch_plain_t(const KParams &kp, int threads, int blocks_per_sm, cudaStream_t s,
                            LaunchShape *out) {
     auto kern = vmc_plain_kernel<R, PROPS, FLU, SKIP, GRAD>;
-    size_t smem = SmemLayout<R>::total(kp.nr, kp.rr_shared, FLU, kp.win_dim);
+    size_t smem = SmemLayout<R>::total(kp.hist_n, FLU, kp.win_dim);
     if (GRAD && kp.fd_n > 0) smem += SmemLayout<R>::fd_bytes(threads);
     cudaError_t e;
     if (smem > 48 * 1024) {

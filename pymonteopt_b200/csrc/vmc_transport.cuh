@@ -122,12 +122,13 @@ struct SmemLayout {
     static constexpr size_t valid_off = cnt_off + PMO_COUNTERS_N * sizeof(unsigned long long);
     static constexpr size_t gl_off = valid_off + 256;  // per-label gradient sums
     static constexpr size_t rr_off = gl_off + 2 * 256 * sizeof(double);
-    __host__ __device__ static size_t win_off(int nr, int rr_shared) {
-        size_t o = rr_off + (rr_shared ? (size_t)PMO_RR_CATS * nr * sizeof(R) : 0);
+    // privatised exit histograms (hist_n entries), then the fluence window
+    __host__ __device__ static size_t win_off(int hist_n) {
+        size_t o = rr_off + (size_t)hist_n * sizeof(R);
         return (o + 15) & ~size_t(15);
     }
-    __host__ __device__ static size_t total(int nr, int rr_shared, int flu, const int32_t win_dim[3]) {
-        size_t o = win_off(nr, rr_shared);
+    __host__ __device__ static size_t total(int hist_n, int flu, const int32_t win_dim[3]) {
+        size_t o = win_off(hist_n);
         if (flu == PMO_FLU_SHARED)
             o += (size_t)win_dim[0] * win_dim[1] * win_dim[2] * sizeof(unsigned long long);
         return (o + 15) & ~size_t(15);
@@ -169,11 +170,13 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
     double *s_gma = reinterpret_cast<double *>(smem_raw + L::gl_off);
     double *s_gms = s_gma + 256;
     unsigned long long *s_win =
-        reinterpret_cast<unsigned long long *>(smem_raw + L::win_off(kp.nr, kp.rr_shared));
+        reinterpret_cast<unsigned long long *>(smem_raw + L::win_off(kp.hist_n));
+    R *s_ang = s_rr + PMO_RR_CATS * kp.nr;    // with rr_shared: 2 x n_ang
+    R *s_line = s_ang + 2 * kp.n_ang;         // and n_line
     const int n_win = FLU == PMO_FLU_SHARED ? kp.win_dim[0] * kp.win_dim[1] * kp.win_dim[2] : 0;
     const bool fd = GRAD && kp.fd_n > 0;
     double *s_fdsum = reinterpret_cast<double *>(
-        smem_raw + L::total(kp.nr, kp.rr_shared, FLU, kp.win_dim));
+        smem_raw + L::total(kp.hist_n, FLU, kp.win_dim));
     float *s_fdL = reinterpret_cast<float *>(s_fdsum + 2 * PMO_FD_MAX) +
                    threadIdx.x * 2 * PMO_FD_MAX;   // this thread's sum of mu * L per target
     float *s_fdN = s_fdL + PMO_FD_MAX;             // and interaction count per target
@@ -195,8 +198,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
     if (fd)
         for (int i = threadIdx.x; i < 2 * PMO_FD_MAX; i += blockDim.x) s_fdsum[i] = 0.0;
     for (int i = threadIdx.x; i < PMO_COUNTERS_N; i += blockDim.x) s_cnt[i] = 0ull;
-    if (kp.rr_shared)
-        for (int i = threadIdx.x; i < PMO_RR_CATS * kp.nr; i += blockDim.x) s_rr[i] = R(0);
+    for (int i = threadIdx.x; i < kp.hist_n; i += blockDim.x) s_rr[i] = R(0);
     for (int i = threadIdx.x; i < n_win; i += blockDim.x) s_win[i] = 0ull;
     __syncthreads();
 
@@ -395,6 +397,37 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
                         atomicAdd(s_rr + cat * kp.nr + b, (R)w);
                     } else {
                         atomicAdd(kp.rr + cat * kp.nr + b, (float)w);
+                    }
+                }
+            }
+        }
+        if (!GRAD && kp.n_ang > 0 && vz != R(0)) {
+            // arccos|v_z| in bins (i da, (i+1) da] (pymopt/metrics/_scoring.py:27-38);
+            // a normal exit (angle 0) falls in no bin, as there
+            const float at = acosf(fminf(fabsf((float)vz), 1.f));
+            if (at > 0.f) {
+                const int b = (int)ceilf(at * kp.inv_da) - 1;
+                if (b >= 0 && b < kp.n_ang) {
+                    const int i = (vz < R(0) ? 0 : kp.n_ang) + b;
+                    if (kp.rr_shared) atomicAdd(s_ang + i, (R)w);
+                    else atomicAdd(kp.ang + i, (float)w);
+                }
+            }
+        }
+        if (!GRAD && kp.n_line > 0 && vx < R(0)) {
+            // exit depth profile of photons moving towards -x within
+            // |y| < y_range (pymopt/metrics/_scoring.py:40-51), with the
+            // model's z encoding rounded to 1e-6 mm
+            // (pymopt/voxel_gpu/_classes.py:302-310)
+            const double ld = (double)kp.l;
+            const double y = ld * (double)(iy - kp.cy) + (double)py;
+            if (fabs(y) < (double)kp.line_y) {
+                const double z = rint((ld * (double)(iz - 1) + (double)pz + ld / 2) * 1e6) / 1e6;
+                if (z > 0.0) {
+                    const int b = (int)ceil(z / (double)kp.line_dr) - 1;
+                    if (b >= 0 && b < kp.n_line) {
+                        if (kp.rr_shared) atomicAdd(s_line + b, (R)w);
+                        else atomicAdd(kp.line + b, (float)w);
                     }
                 }
             }
@@ -801,9 +834,16 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
         if (s_led[i] != 0.0) atomicAdd(kp.ledger + i, s_led[i]);
     for (int i = threadIdx.x; i < PMO_COUNTERS_N; i += blockDim.x)
         if (s_cnt[i] != 0ull) atomicAdd(kp.counters + i, s_cnt[i]);
-    if (kp.rr_shared)
-        for (int i = threadIdx.x; i < PMO_RR_CATS * kp.nr; i += blockDim.x)
-            if (s_rr[i] != R(0)) atomicAdd(kp.rr + i, (float)s_rr[i]);
+    if (kp.rr_shared) {
+        const int n_rr = PMO_RR_CATS * kp.nr, n_ang2 = 2 * kp.n_ang;
+        for (int i = threadIdx.x; i < kp.hist_n; i += blockDim.x) {
+            if (s_rr[i] == R(0)) continue;
+            float *dst = i < n_rr ? kp.rr + i
+                                  : (i < n_rr + n_ang2 ? kp.ang + (i - n_rr)
+                                                       : kp.line + (i - n_rr - n_ang2));
+            atomicAdd(dst, (float)s_rr[i]);
+        }
+    }
     if (fd)
         for (int i = threadIdx.x; i < 2 * kp.fd_n; i += blockDim.x)
             if (s_fdsum[i] != 0.0) atomicAdd(kp.fd_out + i, s_fdsum[i]);

@@ -119,6 +119,12 @@ class TallySpec:
     window: Optional[tuple] = None      # ((lo_x, lo_y, lo_z), (dim_x, dim_y, dim_z))
     export_exits: bool = False
     photon_stats: bool = False
+    # angle-resolved exits: bins of arccos|v_z| over [0, pi/2]
+    n_ang: int = 0
+    # line profile of exits moving towards -x: depth bins for |y| < line_y_range
+    n_line: int = 0
+    line_dr: float = 0.1
+    line_y_range: float = 5.0
 
 
 class Tallies:
@@ -137,6 +143,10 @@ class Tallies:
         # per unit weight; int64 storage of the kernel's unsigned sums)
         self.absorbed = (torch.zeros(dprob.labels.shape, dtype=torch.int64, device=dev)
                          if spec.fluence != A.PMO_FLU_NONE else None)
+        self.ang = (torch.zeros(2, spec.n_ang, dtype=torch.float32, device=dev)
+                    if spec.n_ang > 0 else None)
+        self.line = (torch.zeros(spec.n_line, dtype=torch.float32, device=dev)
+                     if spec.n_line > 0 else None)
         N = self.capacity
         if spec.export_exits:
             self.exit_add = torch.zeros(3, N, dtype=torch.int32, device=dev)
@@ -151,7 +161,7 @@ class Tallies:
             self.ph = None
 
     def zero_(self) -> "Tallies":
-        for t in (self.ledger, self.counters, self.rr, self.absorbed):
+        for t in (self.ledger, self.counters, self.rr, self.absorbed, self.ang, self.line):
             if t is not None:
                 t.zero_()
         self.n_photons = 0
@@ -174,6 +184,9 @@ class Tallies:
                 t.win_dim[a] = int(dim[a])
         t.exit_add, t.exit_p = _ptr(self.exit_add), _ptr(self.exit_p)
         t.exit_v, t.exit_w = _ptr(self.exit_v), _ptr(self.exit_w)
+        t.ang, t.n_ang = _ptr(self.ang), int(sp.n_ang)
+        t.line, t.n_line = _ptr(self.line), int(sp.n_line)
+        t.line_dr, t.line_y_range = float(sp.line_dr), float(sp.line_y_range)
         if self.ph is not None:
             t.ph_interact = self.ph[0].data_ptr()
             t.ph_cross = self.ph[1].data_ptr()

@@ -423,6 +423,9 @@ class BaseVoxelMonteCarlo(metaclass=ABCMeta):
     Extra keywords beyond the reference's:
     ``nr``, ``dr`` — on-device R(r)/T(r) bins (bins (i*dr, (i+1)*dr], mm);
     ``fluence`` — tally absorbed weight per voxel for :meth:`get_fluence`;
+    ``n_ang`` — on-device angle-resolved exit bins for :meth:`get_Ra` /
+    :meth:`get_Ta`; ``n_line``, ``line_dr``, ``line_y_range`` — on-device
+    side-face line profile for :meth:`get_line_profile`;
     ``keep_exits`` — export per-photon exit states for :meth:`get_result`
     (None: on when nPh <= 1e7); ``precision`` — 'fp32' (product) or 'fp64';
     ``verbose`` — the reference's progress prints.
@@ -432,6 +435,7 @@ class BaseVoxelMonteCarlo(metaclass=ABCMeta):
     def __init__(self, *, nPh, model, dtype_f=np.float32, dtype=np.int32,
                  beam_type="TEM00", w_beam=0, beam_angle=0, initial_refrect_by_angle=False,
                  first_layer_clear=False, threadnum=128, nr=100, dr=0.1, fluence=False,
+                 n_ang=0, n_line=0, line_dr=0.1, line_y_range=5.0,
                  keep_exits=None, precision="fp32", verbose=True, device=None):
         def __check_list_name(name, name_list):
             if name not in name_list:
@@ -454,6 +458,10 @@ class BaseVoxelMonteCarlo(metaclass=ABCMeta):
         self.threadnum = int(threadnum)
         self.nr = int(nr)
         self.dr = float(dr)
+        self.n_ang = int(n_ang)
+        self.n_line = int(n_line)
+        self.line_dr = float(line_dr)
+        self.line_y_range = float(line_y_range)
         self.fluence = bool(fluence)
         self.fluence_mode = "voxel" if fluence else False
         self.keep_exits = keep_exits
@@ -562,7 +570,8 @@ class BaseVoxelMonteCarlo(metaclass=ABCMeta):
         keep = self.keep_exits if self.keep_exits is not None else self.nPh <= 10_000_000
         spec = E.TallySpec(nr=self.nr, dr=self.dr,
                            fluence=A.PMO_FLU_GLOBAL if self.fluence else A.PMO_FLU_NONE,
-                           export_exits=bool(keep))
+                           export_exits=bool(keep), n_ang=self.n_ang, n_line=self.n_line,
+                           line_dr=self.line_dr, line_y_range=self.line_y_range)
         if self.verbose:
             print("")
             print("###### Start (Random seed: %s) ######" % rand_seed)
@@ -697,6 +706,37 @@ class BaseVoxelMonteCarlo(metaclass=ABCMeta):
 
     def get_Tr(self, surface_only=False):
         return self._profile((A.PMO_RR_BOTTOM, A.PMO_RR_LAT_POS), surface_only)
+
+    def _angular(self, row):
+        if self._tallies is None or self._tallies.ang is None:
+            raise RuntimeError("construct the model with n_ang > 0 for angle-resolved exits")
+        nn = self.n_ang
+        da = np.pi / (2 * nn)
+        alpha = np.array([(i + 0.5) * da for i in range(nn + 1)])
+        do = 4 * np.pi * np.sin(alpha) * np.sin(da / 2)
+        h = self._tallies.ang[row].cpu().numpy().astype(np.float64)
+        return alpha[:-1], h / (do[:-1] * self.nPh)
+
+    def get_Ra(self):
+        """Angle-resolved reflectance of exits with v_z < 0 [sr^-1], as
+        metrics.angularyResolved on them (pymopt/metrics/_scoring.py:27-38)."""
+        return self._angular(0)
+
+    def get_Ta(self):
+        """Angle-resolved transmittance of exits with v_z > 0 [sr^-1]."""
+        return self._angular(1)
+
+    def get_line_profile(self):
+        """Depth profile [mm^-2] of exits moving towards -x within
+        |y| < line_y_range, as metrics.lineDistance on them
+        (pymopt/metrics/_scoring.py:40-51; pymopt/virtualOBD.py:171-172)."""
+        if self._tallies is None or self._tallies.line is None:
+            raise RuntimeError("construct the model with n_line > 0 for the line profile")
+        nn, dr = self.n_line, self.line_dr
+        alpha = np.array([i * dr for i in range(nn + 1)])
+        da = np.ones(nn) * dr * self.line_y_range * 2
+        h = self._tallies.line.cpu().numpy().astype(np.float64)
+        return alpha[:-1], h / (da * self.nPh)
 
     def get_fluence(self):
         """Fluence per voxel of the interior (shell stripped), FP64:

@@ -1,0 +1,68 @@
+"""On-device angle-resolved and line-profile exit tallies.
+
+Each device histogram is checked against the host restatement of the
+reference's scoring (``pymonteopt_b200.metrics``, itself checked against the
+reference's functions in ``tests/test_host_api.py``).  That restatement runs
+on the exit states the same run exports:
+
+* R(alpha)/T(alpha): ``angularyResolved`` over the exits with v_z < 0 / v_z > 0
+  (pymopt/metrics/_scoring.py:27-38);
+* the side-face line profile: ``lineDistance`` over the exits with v_x < 0
+  (pymopt/metrics/_scoring.py:40-51, as pymopt/virtualOBD.py:171-172 calls it).
+"""
+import numpy as np
+import pytest
+
+from pymonteopt_b200 import VoxelPlateModel
+from pymonteopt_b200 import metrics
+
+pytestmark = pytest.mark.gpu
+
+
+def _model(**kw):
+    m = VoxelPlateModel(nPh=200000, n_ang=30, n_line=60, line_dr=0.05, line_y_range=0.6,
+                        keep_exits=True, verbose=False, **kw)
+    # a narrow slab, so many photons leave through the side faces
+    m.build(x_size=2.0, y_size=2.0, voxel_space=0.05, thickness=[1.0, 1.0], n=[1.37, 1.45],
+            n_air=1.0, ma=[0.1, 0.05], ms=[8.0, 12.0], g=[0.85, 0.9])
+    return m
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp64"])
+def test_angle_resolved_matches_host_scoring(cuda, precision):
+    m = _model(precision=precision).start(rand_seed=9)
+    res = m.get_result()
+    v, w, n = res["v"], res["w"], res["nPh"]
+    for getter, sel in ((m.get_Ra, v[2] < 0), (m.get_Ta, v[2] > 0)):
+        a_dev, dev = getter()
+        a_host, host = metrics.angularyResolved(v[:, sel], w[sel], m.n_ang, n)
+        np.testing.assert_allclose(a_dev, a_host, rtol=0, atol=1e-12)
+        assert host.sum() > 0
+        np.testing.assert_allclose(dev, host, rtol=1e-4, atol=1e-6 * host.max())
+
+
+def test_line_profile_matches_host_scoring(cuda):
+    m = _model().start(rand_seed=10)
+    res = m.get_result()
+    p, v, w, n = res["p"], res["v"], res["w"], res["nPh"]
+    sel = v[0] < 0
+    a_dev, dev = m.get_line_profile()
+    a_host, host = metrics.lineDistance(p[:, sel], w[sel], m.n_line, m.line_dr, n,
+                                        y_range=m.line_y_range)
+    np.testing.assert_allclose(a_dev, a_host, rtol=0, atol=1e-12)
+    assert host.sum() > 0 and np.count_nonzero(host) > 20
+    # exit depths are encoded in single precision on the device and in
+    # double on the host: a photon within 1e-6 mm of a bin edge may change bin
+    np.testing.assert_allclose(dev, host, rtol=2e-3, atol=2e-3 * host.max())
+    assert abs(dev.sum() - host.sum()) <= 1e-3 * host.sum()
+
+
+def test_exit_tallies_off_by_default(cuda):
+    m = VoxelPlateModel(nPh=1000, verbose=False)
+    m.build(x_size=1.0, y_size=1.0, voxel_space=0.1, thickness=[1.0], n=[1.4], n_air=1.0,
+            ma=[0.1], ms=[5.0], g=[0.9])
+    m.start(rand_seed=1)
+    with pytest.raises(RuntimeError):
+        m.get_Ra()
+    with pytest.raises(RuntimeError):
+        m.get_line_profile()
