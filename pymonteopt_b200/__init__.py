@@ -12,5 +12,7 @@ from .voxel import (  # noqa: E402,F401
     VoxelPlateModel,
     VoxelTuringModel,
 )
+from .turing import TuringPattern  # noqa: E402,F401
 
-__all__ = ["VoxelPlateModel", "VoxelPlateExModel", "VoxelTuringModel", "VoxelArrayModel"]
+__all__ = ["VoxelPlateModel", "VoxelPlateExModel", "VoxelTuringModel", "VoxelArrayModel",
+           "TuringPattern"]

@@ -13,6 +13,8 @@ Usage::
 
 The reference imports pydicom, matplotlib and seaborn at module level although
 the transport path never calls them; they are stubbed with empty modules.
+The "turing" case runs the reference's CPU Turing-pattern generator
+(pymopt/modeling/_classes.py) on a small grid.
 The fixtures are committed; nothing at test time needs the reference.
 """
 from __future__ import annotations
@@ -40,6 +42,11 @@ def _stub_modules():
     sys.modules["matplotlib"].pyplot = sys.modules["matplotlib.pyplot"]
     sys.modules["matplotlib"].colors = sys.modules["matplotlib.colors"]
     sys.modules["matplotlib.colors"].LogNorm = object
+    sys.modules["seaborn"].set_style = lambda *a, **k: None
+    for sub in ("pydicom.uid", "pydicom.dataset"):
+        sys.modules.setdefault(sub, types.ModuleType(sub))
+    sys.modules["pydicom.uid"].ImplicitVRLittleEndian = None
+    sys.modules["pydicom.dataset"].Dataset = sys.modules["pydicom.dataset"].FileDataset = object
 
 
 # Plate cases: name -> (params, nPh, seeds, nr, dr).  'c1' is the C1 workload;
@@ -248,11 +255,57 @@ def run_sources_case(ref_root: str) -> str:
     return path
 
 
+# Turing-pattern generator case: small grid, few steps, seeded
+TURING_GEN = dict(grid=8, dx=1 / 8, dt=1, du=0.0002, dv=0.01, length=3, repetition=12,
+                  bv_tv=0.138, voxelsize=0.0295, seed=3, ct_coef=4.5e4, tile_num_xz=1,
+                  tile_num_y=2)
+
+
+def run_turing_case(ref_root: str) -> str:
+    """The reference's CPU Turing-pattern generator (pymopt/modeling/_classes.py,
+    the scipy.fftpack twin of pymopt/modeling_gpu/_classes.py) on a 24^3 grid:
+    the field after the reaction-diffusion steps, the thresholded
+    microarchitecture and the binarised, tiled volume."""
+    import tempfile
+    _stub_modules()
+    sys.path.insert(0, ref_root)
+    from pymopt.modeling import _classes as MC
+    MC.tqdm = lambda it: it
+    tp = MC.TuringPattern()
+    tp.set_params(**TURING_GEN)
+    with contextlib.redirect_stdout(io.StringIO()):
+        tp._calc_kukv()
+        u, v = tp._get_inital_vector()
+        fields = {"u0": u.copy(), "v0": v.copy()}
+        for i in range(tp.repetition):
+            u, v = tp._calc_onestep(u, v)
+            if i == 0:
+                fields["u1"] = u.copy()
+        fields["u_final"] = u.copy()
+        tp2 = MC.TuringPattern()
+        tp2.set_params(**TURING_GEN)
+        with tempfile.TemporaryDirectory(dir=HERE) as d:
+            vol = tp2.modeling(d)
+            with open(os.path.join(d, "_info.json")) as f:
+                info = json.load(f)
+    path = os.path.join(HERE, "ref_turing.npz")
+    micro = info["microarchitecture"]
+    fields.pop("v0")
+    np.savez_compressed(path, volume=vol, threshold=np.float64(tp2.threshold),
+                        micro_keys=np.array(list(micro.keys())),
+                        micro_values=np.array([float(x) for x in micro.values()]),
+                        params_json=np.array(json.dumps(TURING_GEN)), **fields)
+    return path
+
+
 def main():
     ref_root = sys.argv[1]
-    cases = sys.argv[2:] or list(PLATE_CASES) + ["c3", "volumes", "sources"]
+    cases = sys.argv[2:] or list(PLATE_CASES) + ["c3", "volumes", "sources", "turing"]
     for name in cases:
         t0 = time.time()
+        if name == "turing":
+            print("turing ->", run_turing_case(ref_root))
+            continue
         if name == "volumes":
             print("volumes ->", run_volumes_case(ref_root))
             continue
