@@ -322,3 +322,36 @@ def batched_vs_plain(count: int = 4096, plain_sample: int = 48, seed: int = 0, n
         "autotune_seconds": tune_s,
         "max_energy_residual": float(np.max(np.abs(res["balance"]))),
     }
+
+
+def main(argv=None) -> int:
+    """``python -m pymonteopt_b200.batched``: time graph replays of the C5
+    slab batch (forward + gradient) and print one JSON line."""
+    import argparse
+    import json
+    from . import volumes as V
+    ap = argparse.ArgumentParser(description=main.__doc__.split("\n")[0])
+    ap.add_argument("--count", type=int, default=4096, help="slab problems")
+    ap.add_argument("--photon-scale", type=float, default=1.0,
+                    help="multiplies every photon budget")
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--block-threads", type=int, default=0)
+    ap.add_argument("--chunk", type=int, default=0, help="photons per work item")
+    args = ap.parse_args(argv)
+    b = V.c5_slab_batch(seed=0, count=args.count)
+    photons = np.maximum(1, (b["n_photons"] * args.photon_scale).astype(np.int64))
+    sb = SlabBatch(b["ma"], b["ms"], b["g"], b["n"], b["thickness"], photons, nr=32, dr=0.1,
+                   seed=1, autotune=not (args.block_threads and args.chunk),
+                   block_threads=args.block_threads, chunk=args.chunk)
+    tb = time_batch(sb, reps=args.reps)
+    res = sb.fetch()
+    print(json.dumps({"problems": sb.P, "photons": float(photons.sum()),
+                      "seconds": tb["seconds"], "evals_per_s": tb["evals_per_s"],
+                      "photons_per_s": float(photons.sum()) / tb["seconds"],
+                      "block_threads": sb.block_threads, "photons_per_item": sb.chunk,
+                      "max_energy_residual": float(np.max(np.abs(res["balance"])))}))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

@@ -66,3 +66,34 @@ def test_exit_tallies_off_by_default(cuda):
         m.get_Ra()
     with pytest.raises(RuntimeError):
         m.get_line_profile()
+
+
+def test_save_result_writes_reference_format(cuda):
+    """save_result (pymopt/voxel_gpu/_classes.py:338-382): a bz2 pickle of
+    get_result() and an _info.json with the reference's keys."""
+    import bz2
+    import json
+    import os
+    import pickle
+    import tempfile
+    m = VoxelPlateModel(nPh=5000, keep_exits=True, verbose=False)
+    m.build(x_size=1.0, y_size=1.0, voxel_space=0.1, thickness=[1.0], n=[1.4], n_air=1.0,
+            ma=[0.1], ms=[5.0], g=[0.9])
+    m.start(rand_seed=2)
+    res = m.get_result()
+    with tempfile.TemporaryDirectory(dir=os.path.dirname(os.path.abspath(__file__))) as d:
+        base = os.path.join(d, "run")
+        m.save_result(base, coment="check")
+        with bz2.open(base + "_LID.pkl.bz2", "rb") as fp:
+            back = pickle.loads(fp.read())
+        with open(base + "_info.json") as fp:
+            info = json.load(fp)
+    assert set(back) == {"p", "v", "w", "nPh"} and back["nPh"] == 5000
+    for k in ("p", "v", "w"):
+        np.testing.assert_array_equal(back[k], res[k])
+    assert set(info) == {"Date", "coment", "number_of_photons", "calc_dtype", "model", "w_beam",
+                         "beam_angle", "initial_refrect_mode", "beam_mode", "fluence_mode"}
+    assert set(info["model"]) == {"model_name", "model_params", "model_voxel_space",
+                                  "model_xy_size"}
+    assert info["coment"] == "check" and info["number_of_photons"] == 5000
+    assert info["calc_dtype"] == "32 bit" and info["model"]["model_name"] == "PlateModel"
