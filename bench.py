@@ -424,6 +424,21 @@ def main() -> int:
         "mufu_per_photon": opcount.mufu_ops(counters.astype(np.uint64)) / (photons * args.steps),
         "philox_draws_per_photon": opcount.philox_draws(counters.astype(np.uint64)) / (photons * args.steps),
     }
+    if traffic and "warp_inst_per_photon" in traffic:
+        # the instruction-issue ceiling: warp instructions per photon (ncu, same
+        # workload) x photons/s against 4 schedulers x SMs x the sampled clock
+        sms = torch.cuda.get_device_properties(dev).multi_processor_count
+        clk_hz = (clk.get("sm_mhz") or clk.get("sm_max_mhz") or 0) * 1e6
+        ach = traffic["warp_inst_per_photon"] * photons / launch_s
+        pk = 4 * sms * clk_hz
+        roofline["issue"] = {
+            "achieved": ach / 1e9, "peak": pk / 1e9 if pk else None,
+            "unit": "G warp inst/s", "frac": ach / pk if pk else None,
+            "warp_inst_per_photon": traffic["warp_inst_per_photon"],
+            "lanes_per_warp_inst": traffic["thread_inst_per_photon"] / traffic["warp_inst_per_photon"],
+            "source": "instruction counts from ncu on the same workload (profiles/vmc_plain_c2_ncu.json); "
+                      "peak = 4 issue slots x SMs x median sampled SM clock",
+        }
     inflow = ledger[A.PMO_L_WINIT] + ledger[A.PMO_L_RGAIN]
     outflow = (ledger[A.PMO_L_RD] + ledger[A.PMO_L_TT] + ledger[A.PMO_L_EXIT0] +
                ledger[A.PMO_L_ABS] + ledger[A.PMO_L_RLOSS] + ledger[A.PMO_L_ERRW])
