@@ -348,6 +348,7 @@ def main() -> int:
     from pymonteopt_b200 import _abi as A
     from pymonteopt_b200 import engine as E
     from pymonteopt_b200 import opcount
+    from pymonteopt_b200 import replicas
     from pymonteopt_b200 import volumes as V
     from pymonteopt_b200._lib import load
 
@@ -362,7 +363,8 @@ def main() -> int:
     prob = V.c2_skin()
     dp = E.DeviceProblem(prob, dev)
     spec = E.TallySpec(nr=100, dr=0.1)
-    begin0 = rank * photons * (args.steps + args.warmup + 1)
+    # disjoint photon ids for every rank and launch (replicas of one problem)
+    begin0 = replicas.rank_offset(rank, photons, args.steps + args.warmup + 1)
 
     def step(k: int, tallies):
         return E.run_plain(dp, photons, seed=1000 + k, tallies=tallies,
@@ -400,10 +402,7 @@ def main() -> int:
     dev_s = sum(a.elapsed_time(b) for a, b in evs) / 1e3
     for t in tallies:
         t.check()
-    t_max = torch.tensor([dev_s], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
-    dev_s_max = float(t_max.item())
+    dev_s_max = replicas.max_over_ranks(dev_s, dev)
     total_photons = photons * args.steps * world
     value = total_photons / dev_s_max
 
@@ -479,11 +478,8 @@ def main() -> int:
             host_cnt.copy_(et.counters, non_blocking=True)
             e_ev[k][1].record(stream)
         torch.cuda.synchronize()
-        e_s = torch.tensor([sum(a.elapsed_time(b) for a, b in e_ev) / 1e3],
-                           dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(e_s, op=dist.ReduceOp.MAX)
-        e2e = {"value": total_photons / float(e_s.item()), "unit": UNIT,
+        e_s = replicas.max_over_ranks(sum(a.elapsed_time(b) for a, b in e_ev) / 1e3, dev)
+        e2e = {"value": total_photons / e_s, "unit": UNIT,
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
 
     batched = None
