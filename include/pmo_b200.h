@@ -113,9 +113,10 @@ typedef struct pmo_problem {
     int32_t nx, ny, nz;
     float voxel_space;           /* l [mm] */
     /* optional uniform-box map from pmo_build_voxel_words (label in the low
-       byte, box radius in the high byte).  With it, photons in per-label
-       optics step from the face of one label-uniform cube to the next instead
-       of from voxel face to voxel face: the same path, fewer crossings.
+       byte, the box's z half-extent and lateral code in the high byte).  With
+       it, photons in per-label optics step from the face of one label-uniform
+       box to the next instead of from voxel face to voxel face: the same
+       path, fewer crossings.
        NULL: voxel-by-voxel stepping exactly as the reference. */
     const uint16_t *voxel_words;
     int32_t end_label;           /* shell label; photons leave when they enter it */
@@ -418,11 +419,19 @@ int pmo_philox_words_curand(unsigned long long seed,
    denominator of the FP32-issue roofline.  No counterpart in the reference. */
 int pmo_fp32_probe(float *out, int blocks, int threads, int iters, void *stream);
 
-/* Uniform-box map of a label volume: words[i] = labels[i] | R << 8 where R
-   (1 .. cap+1) is the Chebyshev distance from voxel i to the nearest voxel
-   of another label (array border counted as a label change).  scratch:
-   2 * nx*ny*nz bytes of device memory.  No counterpart in the reference,
-   which steps voxel by voxel (pymopt/voxel_gpu/_cukernel.py:77-176). */
+/* Uniform-box map of a label volume.  words[i] = labels[i] | d << 8 | c << 12
+   describes a box {|dx|, |dy| <= e, |dz| <= d} of voxels around voxel i that
+   all carry labels[i] and lie inside the array:
+   - d (0 .. cap, cap <= 15) is the Chebyshev distance from voxel i to the
+     nearest voxel with a 26-neighbour of another label (array border
+     counted as such);
+   - e = max(d, lat(c)) with lat(0) = 0 and
+     lat(c) = ((2 | (c & 1)) << (c >> 1)) >> 1 (1, 2, 3, 4, 6, ... 192);
+   - c is the largest code whose lat(c) does not exceed the smallest
+     in-plane uniform radius over the box's z-planes.
+   scratch: 3 * nx*ny*nz bytes of device memory.  No counterpart in the
+   reference, which steps voxel by voxel
+   (pymopt/voxel_gpu/_cukernel.py:77-176). */
 int pmo_build_voxel_words(const uint8_t *labels, int nx, int ny, int nz, int cap,
                           uint16_t *words, void *scratch, size_t scratch_bytes,
                           void *stream);

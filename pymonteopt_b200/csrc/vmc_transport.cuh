@@ -102,6 +102,16 @@ __device__ __forceinline__ unsigned long long to_fixed(double dw) {
     return __double2ull_rn(dw * (double)(1ull << PMO_ABSORBED_SHIFT));
 }
 
+// Box half-extents (voxels) of a uniform-box map word: z half-extent d in
+// bits 8-11, lateral code c in bits 12-15 with lateral half-extent
+// max(d, lat(c)), lat(0) = 0, lat(c) = ((2 | (c & 1)) << (c >> 1)) >> 1.
+__device__ __forceinline__ void box_extents(uint32_t word, int &bz, int &bl) {
+    bz = (int)((word >> 8) & 0xfu);
+    const int c = (int)(word >> 12);
+    const int lat = c ? ((2 | (c & 1)) << (c >> 1)) >> 1 : 0;
+    bl = lat > bz ? lat : bz;
+}
+
 // theta(g, rand) of the reference (pymopt/voxel_gpu/_cukernel.py:14-25)
 template <typename R>
 __device__ __forceinline__ R hg_cos(const LabelProps<R> &t, R u) {
@@ -216,15 +226,16 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
     // thread totals, reduced once at the end
     double t_abs = 0.0;
 
-    // photon state (registers).  The photon sits in a label-uniform box of
-    // (2 rad - 1)^3 voxels centred on voxel (ix, iy, iz) with linear index
-    // lin; (px, py, pz) is its offset from that voxel's centre and hw the
-    // box half-width.  rad == 1 is the reference's voxel-by-voxel stepping.
+    // photon state (registers).  The photon sits in a label-uniform box
+    // {|dx|, |dy| <= bl, |dz| <= bz} (voxels) around voxel (ix, iy, iz) with
+    // linear index lin; (px, py, pz) is its offset from that voxel's centre,
+    // hwl and hwz the box's lateral and z half-widths.  bl == bz == 0 is the
+    // reference's voxel-by-voxel stepping.
     uint64_t pid = 0;
-    int ix = 0, iy = 0, iz = 0, lab = 0, rad = 1;
+    int ix = 0, iy = 0, iz = 0, lab = 0, bz = 0, bl = 0;
     uint32_t lin = 0;
     R px = 0, py = 0, pz = 0, vx = 0, vy = 0, vz = 0, ivx = 0, ivy = 0, ivz = 0, w = 0;
-    R hw = 0;
+    R hwl = 0, hwz = 0;
     R mt = 0, imt = 0, ma_mt = 0, ni = 1;
     uint32_t k = 0, f = 0, ncr = 0;
     // the current interaction's draws, kept while its step crosses faces
@@ -244,18 +255,23 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
         pend_q = 0ull;
         pend_lin = 0xffffffffu;
     };
-    // offset of the voxel holding the photon from the box centre, in voxels
-    auto box_k = [&](R q) -> int {
-        const int m = rad - 1;
+    // offset of the voxel holding the photon from the box centre along an
+    // axis of half-extent m, in voxels
+    auto box_k = [&](R q, int m) -> int {
         int k = (int)rint(xmul(q, inv_l));
         return k < -m ? -m : (k > m ? m : k);
+    };
+    auto set_box = [&](uint32_t word) {
+        box_extents(word, bz, bl);
+        hwz = xfma((R)bz, l, hl);
+        hwl = xfma((R)bl, l, hl);
     };
     auto deposit = [&](R dw) {
         const unsigned long long q = to_fixed(dw);
         int cx = ix, cy = iy, cz = iz;
         uint32_t clin = lin;
-        if (SKIP && rad > 1) {
-            const int kx = box_k(px), ky = box_k(py), kz = box_k(pz);
+        if (SKIP && bl > 0) {
+            const int kx = box_k(px, bl), ky = box_k(py, bl), kz = box_k(pz, bz);
             // a map from pmo_build_voxel_words keeps every box inside the
             // array; a caller-supplied map that does not loses the deposit
             // to the box centre instead of writing outside the grid
@@ -544,12 +560,12 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
         if (SKIP) {
             const uint32_t word = __ldg(kp.words + lin);
             lab = (int)(word & 0xffu);
-            rad = (int)(word >> 8);
+            set_box(word);
         } else {
             lab = __ldg(kp.labels + lin);
-            rad = 1;
+            bz = bl = 0;
+            hwz = hwl = hl;
         }
-        hw = xfma((R)rad, l, -hl);
         if (!s_valid[lab]) {
             fail(PMO_C_ERR_LABEL);
             return false;
@@ -577,9 +593,9 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
         int budget = kCrossPerIter;
         for (;;) {
             // distance to the nearest face; db starts at 1000 (:80-90)
-            const R dx = xmul(xsub(copysign(hw, vx), px), ivx);
-            const R dy = xmul(xsub(copysign(hw, vy), py), ivy);
-            const R dz = xmul(xsub(copysign(hw, vz), pz), ivz);
+            const R dx = xmul(xsub(copysign(hwl, vx), px), ivx);
+            const R dy = xmul(xsub(copysign(hwl, vy), py), ivy);
+            const R dz = xmul(xsub(copysign(hwz, vz), pz), ivz);
             R db = R(1000);
             int ax = 0;
             if (dx < db) { db = dx; ax = 0; }
@@ -603,7 +619,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             pz = xfma(vz, db, pz);
             if (GRAD) gL += (float)db;
             const R va = ax == 0 ? vx : (ax == 1 ? vy : vz);
-            const R face = copysign(hw, va);
+            const R face = copysign(ax == 2 ? hwz : hwl, va);
             if (ax == 0) px = face;
             else if (ax == 1) py = face;
             else pz = face;
@@ -612,15 +628,16 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             if (ncr + k - 1 > cap) { fail(PMO_C_ERR_CAP); return false; }
             const bool neg = signbit(va);
             // the voxel of the box that touches this face, and the photon's
-            // offset inside it (for rad == 1: the box itself)
+            // offset inside it (for a one-voxel box: the box itself)
             int cx = ix, cy = iy, cz = iz;
             uint32_t clin = lin;
             R fx = px, fy = py, fz = pz;
-            if (SKIP && rad > 1) {
-                const int m = neg ? -(rad - 1) : rad - 1;
-                const int kx = ax == 0 ? m : box_k(px);
-                const int ky = ax == 1 ? m : box_k(py);
-                const int kz = ax == 2 ? m : box_k(pz);
+            if (SKIP && bl > 0) {
+                const int ma = ax == 2 ? bz : bl;
+                const int m = neg ? -ma : ma;
+                const int kx = ax == 0 ? m : box_k(px, bl);
+                const int ky = ax == 1 ? m : box_k(py, bl);
+                const int kz = ax == 2 ? m : box_k(pz, bz);
                 fx = ax == 0 ? copysign(hl, va) : xfma(-(R)kx, l, px);
                 fy = ax == 1 ? copysign(hl, va) : xfma(-(R)ky, l, py);
                 fz = ax == 2 ? copysign(hl, va) : xfma(-(R)kz, l, pz);
@@ -640,11 +657,11 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             if ((unsigned)nc >= (unsigned)dim) { fail(PMO_C_ERR_GEOM); return false; }
             const uint32_t stride = ax == 0 ? kp.sx : (ax == 1 ? kp.sy : 1u);
             const uint32_t nlin = neg ? clin - stride : clin + stride;
-            int nlab, nrad = 1;
+            int nlab;
+            uint32_t nword = 0;
             if (SKIP) {
-                const uint32_t word = __ldg(kp.words + nlin);
-                nlab = (int)(word & 0xffu);
-                nrad = (int)(word >> 8);
+                nword = __ldg(kp.words + nlin);
+                nlab = (int)(nword & 0xffu);
             } else {
                 nlab = __ldg(kp.labels + nlin);
             }
@@ -658,8 +675,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
                 py = ax == 1 ? -fy : fy;
                 pz = ax == 2 ? -fz : fz;
                 lin = nlin;
-                rad = nrad;
-                hw = xfma((R)rad, l, -hl);
+                if (SKIP) set_box(nword);
             };
             if (PROPS == PMO_PROPS_LABEL && nlab == lab) {
                 // same label on the other side: same n and mu (:154-167)

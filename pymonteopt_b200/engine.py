@@ -37,7 +37,7 @@ def require_cuda(device=None) -> torch.device:
     return d
 
 
-SKIP_CAP = 31   # uniform boxes of up to (2*32 - 1)^3 voxels
+SKIP_CAP = 15   # z half-extent of the uniform boxes (lateral: up to 192 voxels)
 
 
 class DeviceProblem:
@@ -74,7 +74,7 @@ class DeviceProblem:
 
     def build_words(self, stream=None) -> None:
         """(Re)build the uniform-box map from the resident labels."""
-        scratch = torch.empty(2 * self.labels.numel(), dtype=torch.uint8, device=self.device)
+        scratch = torch.empty(3 * self.labels.numel(), dtype=torch.uint8, device=self.device)
         nx, ny, nz = self.labels.shape
         st = load().pmo_build_voxel_words(self.labels.data_ptr(), nx, ny, nz, self.skip_cap,
                                           self.words.data_ptr(), scratch.data_ptr(),

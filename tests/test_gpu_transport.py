@@ -116,43 +116,81 @@ def test_fp64_build_matches_oracle_per_photon(cuda, case):
         assert abs(L[k] - ref["ledger"][k]) <= 0.005 * n, (k, L[k], ref["ledger"][k])
 
 
+def _lat(c):
+    return ((2 | (c & 1)) << (c >> 1)) >> 1 if c else 0
+
+
 def _voxel_words_brute(labels, cap):
-    """R = min(cap, Chebyshev distance to the nearest other label or to the
-    array border) + 1, by brute force (small volumes only)."""
+    """Per voxel, by brute force (small volumes only): d = min(cap, Chebyshev
+    distance to the nearest other label - 1, distance to the array border),
+    and P = the same inside the voxel's z-plane (lateral border only), capped
+    at 192."""
     nx, ny, nz = labels.shape
-    out = np.zeros(labels.shape, np.int64)
+    d = np.zeros(labels.shape, np.int64)
+    P = np.zeros(labels.shape, np.int64)
     idx = np.indices(labels.shape).reshape(3, -1).T
     flat = labels.ravel()
     for i, (x, y, z) in enumerate(idx):
-        d = np.max(np.abs(idx - (x, y, z)), axis=1)
-        other = d[flat != flat[i]]
-        r = other.min() if other.size else cap + 1
-        # the array border counts as a label change
-        r = min(r, x + 1, y + 1, z + 1, nx - x, ny - y, nz - z)
-        out[x, y, z] = min(r - 1, cap) + 1
-    return out
+        cheb = np.max(np.abs(idx - (x, y, z)), axis=1)
+        other = cheb[flat != flat[i]]
+        r = other.min() - 1 if other.size else 10**6
+        d[x, y, z] = min(r, cap, x, y, z, nx - 1 - x, ny - 1 - y, nz - 1 - z)
+        plane = (idx[:, 2] == z) & (flat != flat[i])
+        k = np.max(np.abs(idx[plane][:, :2] - (x, y)), axis=1)
+        q = k.min() - 1 if k.size else 10**6
+        P[x, y, z] = min(q, 192, x, y, nx - 1 - x, ny - 1 - y)
+    return d, P
 
 
-@pytest.mark.parametrize("cap", [2, 31])
-def test_voxel_words_match_brute_force(cuda, cap):
-    rng = np.random.default_rng(5)
-    lab = np.zeros((14, 12, 16), np.uint8)
-    lab[3:11, 2:10, 4:14] = 1
-    lab[5:8, 4:7, 6:9] = 2
-    lab[rng.random(lab.shape) < 0.01] = 3
+def _build_words(lab, cap, cuda):
     d_lab = torch.from_numpy(lab).to(cuda)
     words = torch.empty(lab.shape, dtype=torch.int16, device=cuda)
-    scratch = torch.empty(2 * lab.size, dtype=torch.uint8, device=cuda)
+    scratch = torch.empty(3 * lab.size, dtype=torch.uint8, device=cuda)
     st = load().pmo_build_voxel_words(d_lab.data_ptr(), *lab.shape, cap, words.data_ptr(),
                                       scratch.data_ptr(), scratch.numel(),
                                       torch.cuda.current_stream().cuda_stream)
     assert st == 0
-    w = words.cpu().numpy().view(np.uint16)
+    return words.cpu().numpy().view(np.uint16).astype(np.int64)
+
+
+@pytest.mark.parametrize("cap", [2, 15])
+@pytest.mark.parametrize("volume", ["blocks", "thin_layers"])
+def test_voxel_words_match_brute_force(cuda, cap, volume):
+    rng = np.random.default_rng(5)
+    if volume == "blocks":
+        lab = np.zeros((14, 12, 16), np.uint8)
+        lab[3:11, 2:10, 4:14] = 1
+        lab[5:8, 4:7, 6:9] = 2
+        lab[rng.random(lab.shape) < 0.01] = 3
+    else:
+        # a plate: 1-voxel and 2-voxel layers between thicker ones, shell 4
+        lab = np.full((20, 18, 14), 4, np.uint8)
+        lab[1:-1, 1:-1, 1:3] = 0
+        lab[1:-1, 1:-1, 3:4] = 1
+        lab[1:-1, 1:-1, 4:12] = 2
+        lab[1:-1, 1:-1, 12:13] = 3
+    w = _build_words(lab, cap, cuda)
     assert np.array_equal(w & 0xFF, lab)
-    brute = _voxel_words_brute(lab, cap)
-    # edge voxels (a 26-neighbour of another label) get R = 1 exactly; elsewhere
-    # R is the brute-force Chebyshev radius
-    assert np.array_equal((w >> 8).astype(np.int64), brute)
+    d, P = _voxel_words_brute(lab, cap)
+    wd, wc = (w >> 8) & 0xF, w >> 12
+    assert np.array_equal(wd, d)
+    nx, ny, nz = lab.shape
+    for x in range(nx):
+        for y in range(ny):
+            for z in range(nz):
+                dd = d[x, y, z]
+                e_true = P[x, y, z - dd:z + dd + 1].min()
+                c = max(c for c in range(16) if _lat(c) <= e_true)
+                assert wc[x, y, z] == c, (x, y, z, wc[x, y, z], c, e_true)
+                # the box the kernel will use is inside the array and uniform
+                e = max(dd, _lat(c))
+                assert x - e >= 0 and y - e >= 0 and z - dd >= 0
+                assert x + e < nx and y + e < ny and z + dd < nz
+                box = lab[x - e:x + e + 1, y - e:y + e + 1, z - dd:z + dd + 1]
+                assert np.all(box == lab[x, y, z]), (x, y, z, e, dd)
+    if volume == "thin_layers":
+        # the 1-voxel layer has d = 0 but a lateral reach of several voxels
+        assert wd[10, 9, 3] == 0 and _lat(wc[10, 9, 3]) >= 6
 
 
 @pytest.mark.parametrize("case", ["c1_small", "three_layer", "c3_small"])
