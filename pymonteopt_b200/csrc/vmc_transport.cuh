@@ -236,6 +236,11 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
     uint32_t lin = 0;
     R px = 0, py = 0, pz = 0, vx = 0, vy = 0, vz = 0, ivx = 0, ivy = 0, ivz = 0, w = 0;
     R hwl = 0, hwz = 0;
+    // weight at the start of the current absorption segment (photon start or
+    // the last roulette gain): the segment's absorbed weight is wseg - w, the
+    // exact sum of its implicit-capture decrements (each a difference of two
+    // floats, exact in double, telescoping)
+    R wseg = 0;
     R mt = 0, imt = 0, ma_mt = 0, ni = 1;
     uint32_t k = 0, f = 0, ncr = 0;
     // the current interaction's draws, kept while its step crosses faces
@@ -348,6 +353,8 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
     };
     // photon end: per-photon outputs and counters
     auto finish = [&]() {
+        t_abs += (double)wseg - (double)w;
+        wseg = w;
         if (FLU != PMO_FLU_NONE) deposit_flush();
         // a replayed photon that ends without a binned exit left the forward path
         if (GRAD && ecode < 0) atomicAdd(kp.gcounters + PMO_G_MISMATCH, 1ull);
@@ -542,6 +549,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
                     vy = (R)kp.spec_v[1];
                     vz = (R)kp.spec_v[2];
                     w = R(1);
+                    wseg = w;
                     atomicAdd(s_led + PMO_L_SPEC, 1.0);
                     if (vz < R(0)) atomicAdd(s_led + PMO_L_RD, 1.0);
                     else if (vz > R(0)) atomicAdd(s_led + PMO_L_TT, 1.0);
@@ -550,6 +558,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
                 }
             }
         }
+        wseg = w;
         atomicAdd(s_led + PMO_L_WINIT, (double)w);
         if ((unsigned)ix >= (unsigned)kp.nx || (unsigned)iy >= (unsigned)kp.ny ||
             (unsigned)iz >= (unsigned)kp.nz) {
@@ -753,17 +762,16 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
         // absorption by implicit capture (:179)
         {
             const R wn = xfma(-w, ma_mt, w);
-            const double dw = (double)w - (double)wn;
+            if (FLU != PMO_FLU_NONE) deposit(xsub(w, wn));
             w = wn;
-            t_abs += dw;
-            if (FLU != PMO_FLU_NONE) deposit((R)dw);
         }
         // Russian roulette (:182-195)
         if (w <= R(0.0001)) {
             atomicAdd(s_cnt + PMO_C_ROULETTE, 1ull);
+            t_abs += (double)wseg - (double)w;
             if (R(0.1) < u01<R>(ry)) {
                 atomicAdd(s_led + PMO_L_RLOSS, (double)w);
-                w = R(0);
+                w = wseg = R(0);
                 px = py = pz = R(0);
                 vx = vy = vz = R(0);
                 ix = iy = iz = 0;
@@ -772,7 +780,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             }
             const R wn = xmul(w, R(10));
             atomicAdd(s_led + PMO_L_RGAIN, (double)wn - (double)w);
-            w = wn;
+            w = wseg = wn;
         }
         // scattering: HG polar angle, uniform azimuth, rotation (:197-219)
         {
