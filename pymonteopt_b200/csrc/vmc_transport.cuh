@@ -306,7 +306,12 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             pend_q = q;
         }
     };
+    // The FP64 build keeps 1/v per direction, as the CPU oracle does; the FP32
+    // product divides in place (a * rcp(v), the same value as a * (1/v) with
+    // the approximate divide) and keeps three registers free.
+    constexpr bool kInv = sizeof(R) != sizeof(float);
     auto set_dir_inverse = [&]() {
+        if (!kInv) return;
         ivx = xdiv(R(1), vx);
         ivy = xdiv(R(1), vy);
         ivz = xdiv(R(1), vz);
@@ -602,9 +607,12 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
         int budget = kCrossPerIter;
         for (;;) {
             // distance to the nearest face; db starts at 1000 (:80-90)
-            const R dx = xmul(xsub(copysign(hwl, vx), px), ivx);
-            const R dy = xmul(xsub(copysign(hwl, vy), py), ivy);
-            const R dz = xmul(xsub(copysign(hwz, vz), pz), ivz);
+            const R ax_ = xsub(copysign(hwl, vx), px);
+            const R ay_ = xsub(copysign(hwl, vy), py);
+            const R az_ = xsub(copysign(hwz, vz), pz);
+            const R dx = kInv ? xmul(ax_, ivx) : xdiv(ax_, vx);
+            const R dy = kInv ? xmul(ay_, ivy) : xdiv(ay_, vy);
+            const R dz = kInv ? xmul(az_, ivz) : xdiv(az_, vz);
             R db = R(1000);
             int ax = 0;
             if (dx < db) { db = dx; ax = 0; }
