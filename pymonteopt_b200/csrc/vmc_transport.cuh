@@ -241,13 +241,12 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
     // exact sum of its implicit-capture decrements (each a difference of two
     // floats, exact in double, telescoping)
     R wseg = 0;
-    R mt = 0, imt = 0, ma_mt = 0, ni = 1;
+    R mt = 0, imt = 0, ma_mt = 0;   // of label lab; its index n is s_tab[lab].n
     uint32_t k = 0, f = 0, ncr = 0;
     // the current interaction's draws, kept while its step crosses faces
     uint32_t ry = 0, rz = 0, rw = 0;
     R st = 0;
     bool pending = false;
-    int ecode = -1;                 // exit bin code (category * nr + bin), -1: none
     // gradient replay: q of the photon, path length and sum of 1/mu_s over
     // interactions in the current cell, 1/mu_s of the cell
     float gq = 0.f, gL = 0.f, gN = 0.f, gC = 0.f;
@@ -357,12 +356,13 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
         }
     };
     // photon end: per-photon outputs and counters
-    auto finish = [&]() {
+    // code: the exit's R(r) bin code (category * nr + bin), -1 for none
+    auto finish = [&](int code = -1) {
         t_abs += (double)wseg - (double)w;
         wseg = w;
         if (FLU != PMO_FLU_NONE) deposit_flush();
         // a replayed photon that ends without a binned exit left the forward path
-        if (GRAD && ecode < 0) atomicAdd(kp.gcounters + PMO_G_MISMATCH, 1ull);
+        if (GRAD && code < 0) atomicAdd(kp.gcounters + PMO_G_MISMATCH, 1ull);
         const uint64_t j = pid - kp.begin;
         if (export_exits) {
             kp.exit_add[j] = ix;
@@ -377,7 +377,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             kp.exit_w[j] = (float)w;
         }
         if (score_record) {
-            kp.score_bin[j] = ecode;
+            kp.score_bin[j] = code;
             kp.score_w[j] = (float)w;
         }
         if (photon_stats) {
@@ -398,7 +398,8 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
     // exit into the end label: reference Rd/Tt split by the sign of v_z
     // (pymopt/voxel_gpu/_classes.py:326-334) and radialDistance binning of the
     // encoded exit position (:302-310, pymopt/metrics/_scoring.py:16-25)
-    auto exit_tally = [&](int ax) {
+    auto exit_tally = [&](int ax) -> int {
+        int ecode = -1;
         const double wd = (double)w;
         if (!GRAD)
             atomicAdd(s_led + (vz < R(0) ? PMO_L_RD : (vz > R(0) ? PMO_L_TT : PMO_L_EXIT0)), wd);
@@ -485,6 +486,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             }
         }
         atomicAdd(s_cnt + PMO_C_EXITS, 1ull);
+        return ecode;
     };
 
     // Start photon j: source (pymopt/voxel_gpu/_classes.py:148-254).
@@ -493,7 +495,6 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
         pid = kp.begin + jj;
         k = f = ncr = 0;
         pending = false;
-        ecode = -1;
         if (GRAD) {
             const int code = kp.score_bin[jj];
             gq = code >= 0 ? __ldg(kp.coef + code) * kp.score_w[jj] : 0.f;
@@ -585,7 +586,6 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             return false;
         }
         load_props();
-        ni = s_tab[lab].n;
         set_dir_inverse();
         return true;
     };
@@ -701,6 +701,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             }
             if (nlab != kp.end_label && !s_valid[nlab]) { fail(PMO_C_ERR_LABEL); return false; }
             const R nt = s_tab[nlab].n;
+            const R ni = s_tab[lab].n;
             if (ni != nt) {
                 // Fresnel / total internal reflection (:105-153) with the
                 // cosines and sines of the incidence/transmission angles
@@ -753,10 +754,8 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             // cross (:137-148)
             enter();
             lab = nlab;
-            ni = nt;
             if (lab == kp.end_label) {
-                exit_tally(ax);
-                finish();
+                finish(exit_tally(ax));
                 return false;
             }
             load_props();
