@@ -55,6 +55,8 @@ def parse_args():
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference's own cuVMC kernel on the 256^3 volume")
     ap.add_argument("--ref-gpu-photons", type=float, default=1e7)
+    ap.add_argument("--no-gradient", action="store_true",
+                    help="skip timing the differentiable form (64^3 per-voxel optics)")
     ap.add_argument("--block-threads", type=int, default=0)
     ap.add_argument("--blocks-per-sm", type=int, default=0)
     return ap.parse_args()
@@ -296,6 +298,43 @@ def reference_gpu_leg(torch, dev, photons: int) -> dict:
     return out
 
 
+def gradient_leg(torch, dev, photons: int = 10_000_000, evals: int = 3) -> dict:
+    """The differentiable form on its workload: 64^3 voxels at 0.25 mm with
+    per-voxel optics, 1e7 photons, loss = squared error of the 50-bin R(r)
+    against a seeded target, backward = Philox replay giving dL/dmu_a and
+    dL/dmu_s per voxel.  Times forward and backward with CUDA events."""
+    from pymonteopt_b200 import grad as G
+    from pymonteopt_b200 import volumes as V
+    model = G.DifferentiableRr(V.c4_voxel_props(0), n_photons=photons, seed=3, nr=50, dr=0.1,
+                               props="voxel", device=dev)
+    ma, ms = model.initial_params()
+    target = model(ma * 1.1, ms * 0.95).detach()      # a seeded, different target
+    stream = torch.cuda.current_stream()
+    fw, bw = [], []
+    for k in range(evals + 1):
+        ma_, ms_ = ma.clone().requires_grad_(True), ms.clone().requires_grad_(True)
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        torch.cuda.synchronize()
+        e0.record(stream)
+        R = model(ma_, ms_)
+        loss = ((R - target) ** 2).sum()
+        e1.record(stream)
+        loss.backward()
+        e2.record(stream)
+        torch.cuda.synchronize()
+        if k:                                          # the first evaluation warms up
+            fw.append(e0.elapsed_time(e1) / 1e3)
+            bw.append(e1.elapsed_time(e2) / 1e3)
+    rep = model.last_replay
+    t_f, t_b = float(np.median(fw)), float(np.median(bw))
+    return {"workload": "c4_voxel_props_64^3_per_voxel_optics", "photons": photons,
+            "forward_s": t_f, "backward_s": t_b, "evals_per_s": 1.0 / (t_f + t_b),
+            "forward_photons_per_s": photons / t_f,
+            "replayed_photons": int(rep.replayed), "replay_mismatches": int(rep.mismatches),
+            "backward_replayed_photons_per_s": rep.replayed / t_b,
+            "grad_finite": bool(torch.isfinite(ma_.grad).all() and torch.isfinite(ms_.grad).all())}
+
+
 # ---------------------------------------------------------------------------
 def fp32_probe(torch, lib) -> float:
     """Measured FP32 issue rate (FFMA thread-instructions per second)."""
@@ -493,6 +532,10 @@ def main() -> int:
     if rank == 0 and world == 1 and not args.no_reference_gpu:
         reference_gpu = reference_gpu_leg(torch, dev, int(args.ref_gpu_photons))
 
+    gradient = None
+    if rank == 0 and world == 1 and not args.no_gradient:
+        gradient = gradient_leg(torch, dev)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = cpu_oracle_rate(12.0)
@@ -518,6 +561,7 @@ def main() -> int:
         "gpu_launches": args.steps,
         "batched": batched,
         "reference_gpu": reference_gpu,
+        "gradient": gradient,
         "clocks": clk,
         "wall_s_timed_region": wall,
         "results": results,
