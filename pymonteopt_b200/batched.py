@@ -349,6 +349,8 @@ def main(argv=None) -> int:
                       "seconds": tb["seconds"], "evals_per_s": tb["evals_per_s"],
                       "photons_per_s": float(photons.sum()) / tb["seconds"],
                       "block_threads": sb.block_threads, "photons_per_item": sb.chunk,
+                      "p50_completion_ms": float(np.percentile(res["completion_ms"], 50)),
+                      "p99_completion_ms": float(np.percentile(res["completion_ms"], 99)),
                       "max_energy_residual": float(np.max(np.abs(res["balance"])))}))
     return 0
 
