@@ -400,6 +400,36 @@ int pmo_cuvmc(int32_t *add, float *p, float *v, float *w,
 int pmo_normalize_fluence(const pmo_problem *prob, const unsigned long long *absorbed,
                           double n_photons, double *phi_out, void *stream);
 
+/* ---- optical bench after the transport (pymopt.optics OBD) ---------------- */
+
+/* Element parameters of the reference's OBD and SideOBD
+   (pymopt/optics/_classes.py:381-402, keys of OBD.params; lengths in mm). */
+typedef struct pmo_obd_params {
+    double outer_d1, ct1, r1, n1, bfl1;     /* lens 1 (N-BK7 by default) */
+    double outer_d2, ct2, r2, n2, bfl2;     /* lens 2 (N-SF11 by default) */
+    double slit_d, slit_width, slit_thickness, distance_2slits;
+    double d_pd, pd_correction;             /* photodiode diameter, z offset */
+    int32_t ld_fix_part;                    /* laser-diode mount between the slits */
+    int32_t side;                           /* SideOBD: x shifted by -(Z + side_dz) * side_tan */
+    double side_dz, side_tan;
+    const double *z;                        /* device array: the scan's Z offsets */
+    int32_t n_z;                            /* 1 .. 4096 */
+    uint64_t seed;                          /* Philox key of the Fresnel decisions */
+    double fixed_u;                         /* in [0, 1): use it instead of every
+                                               draw (deterministic); < 0: draw */
+} pmo_obd_params;
+
+/* Intensity at the photodiode for every Z of a scan: intensity[i] +=
+   sum of w over the exit photons (p, v, w: SoA device arrays, 3n/3n/n floats,
+   already selected and prepared as OBD.opticalAnalysisMeth does,
+   pymopt/optics/_classes.py:495-526) that pass lens 1, the slits, the
+   optional mount and lens 2 at detector offset z[i] and land on the
+   photodiode.  Restates the reference's NumPy ray tracing
+   (pymopt/optics/_classes.py:50-380, :454-493, :528-566) per photon;
+   intensity is an FP64 device array of n_z, accumulated. */
+int pmo_run_obd(const pmo_obd_params *prm, const float *p, const float *v, const float *w, int64_t n,
+            double *intensity, void *stream);
+
 /* Philox4x32-10 words of the engine's generator for n counters ctr[4*n]
    (device arrays) under key (key0, key1): known-answer checks of the random
    stream layout.  No counterpart in the reference (it uses cuRAND XORWOW,

@@ -199,5 +199,22 @@ class PmoBatch(C.Structure):
     ]
 
 
+class PmoObdParams(C.Structure):
+    _fields_ = [
+        ("outer_d1", C.c_double), ("ct1", C.c_double), ("r1", C.c_double),
+        ("n1", C.c_double), ("bfl1", C.c_double),
+        ("outer_d2", C.c_double), ("ct2", C.c_double), ("r2", C.c_double),
+        ("n2", C.c_double), ("bfl2", C.c_double),
+        ("slit_d", C.c_double), ("slit_width", C.c_double), ("slit_thickness", C.c_double),
+        ("distance_2slits", C.c_double),
+        ("d_pd", C.c_double), ("pd_correction", C.c_double),
+        ("ld_fix_part", C.c_int32), ("side", C.c_int32),
+        ("side_dz", C.c_double), ("side_tan", C.c_double),
+        ("z", C.c_void_p), ("n_z", C.c_int32),
+        ("seed", C.c_uint64),
+        ("fixed_u", C.c_double),
+    ]
+
+
 class PmoLaunch(C.Structure):
     _fields_ = [("block_threads", C.c_int32), ("blocks_per_sm", C.c_int32)]

@@ -33,6 +33,8 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relax
 PER_FILE = {
     "vmc_plain_f32.cu": ["-ftz=true", "-prec-div=false", "-prec-sqrt=false"],
     "vmc_plain_f64.cu": ["-fmad=false"],
+    # the optical bench rounds every product and sum on its own, like NumPy
+    "obd.cu": ["-fmad=false"],
 }
 DEFAULT_FP = ["-ftz=true", "-prec-div=false", "-prec-sqrt=false"]
 

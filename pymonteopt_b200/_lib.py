@@ -19,6 +19,8 @@ _lib = None
 
 # Every symbol the C header declares, with (restype, argtypes).
 SIGNATURES = {
+    "pmo_run_obd": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64,
+                              C.c_void_p, C.c_void_p]),
     "pmo_abi_version": (C.c_int, []),
     "pmo_status_string": (C.c_char_p, [C.c_int]),
     "pmo_device_info": (C.c_int, [C.POINTER(C.c_int)] * 3),

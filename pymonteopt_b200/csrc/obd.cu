@@ -1,0 +1,248 @@
+// obd.cu — the optical bench that follows the transport: exit photons through
+// a lens, two annular slits, an optional laser-diode mount, a second lens and
+// a photodiode, for every detector offset Z of a scan.
+//
+// This restates the reference's vectorised NumPy ray tracing
+// (pymopt/optics/_classes.py:50-380 for the elements, :454-526 for the
+// scan, :528-566 for the side geometry) per photon:
+// - one thread per exit photon, looping over the scan;
+// - the intensity of each Z summed in shared memory, then one FP64 atomic
+//   per block and Z.
+//
+// Arithmetic follows the reference's NumPy types:
+// - exit photons arrive as float32 and the first normalisation of v runs in
+//   single precision;
+// - every element position depends on Z, a float64 scalar of np.arange, so
+//   from the first plane hit on the positions, normals, directions and
+//   Fresnel terms are float64 (:133-136, :152-222);
+// - the side geometry's shifted x is rounded back to float32, as it is
+//   stored into the float32 array (:561-562);
+// - this file is built without FMA contraction, so products and sums round
+//   one by one as in NumPy.
+//
+// The reference's Fresnel decision at each lens surface is
+// np.random.rand() - R > 0 (:212-215).  Here the four uniforms of a
+// (photon, Z) pair come from one Philox4x32-10 draw, key (seed_lo, seed_hi)
+// and counter (Z index, 5, photon_lo, photon_hi), as x * 2^-32 in [0, 1).
+// A fixed uniform (fixed_u in [0, 1)) replaces the draws for deterministic
+// comparisons.
+#include "pmo_internal.h"
+
+namespace {
+
+struct Ray {
+    double px, py, pz, vx, vy, vz;
+};
+
+__device__ __forceinline__ void normalize(Ray &r) {
+    const double s = sqrt(r.vx * r.vx + r.vy * r.vy + r.vz * r.vz);
+    r.vx = r.vx / s;
+    r.vy = r.vy / s;
+    r.vz = r.vz / s;
+}
+
+// move to the plane z = zp along v (:64-66, :133-136, :325-327)
+__device__ __forceinline__ void hit_plane(Ray &r, double zp) {
+    const double a = (zp - r.pz) / r.vz;
+    r.px = r.px + a * r.vx;
+    r.py = r.py + a * r.vy;
+    r.pz = r.pz + a * r.vz;
+}
+
+__device__ __forceinline__ double radius(const Ray &r) {
+    return sqrt(r.px * r.px + r.py * r.py);
+}
+
+// refraction through a surface with unit normal nn, from air into glass of
+// index n or out of it, with the reference's Fresnel decision u - R > 0
+// (:152-188, :212-222); false: the photon is gone
+__device__ __forceinline__ bool refract(Ray &r, double nx, double ny, double nz, double n,
+                                        bool lens_to_air, double u) {
+    const double cos_ai = nx * r.vx + ny * r.vy + nz * r.vz;
+    const double a = lens_to_air ? n / 1.0 : 1.0 / n;
+    const double ai = acos(cos_ai);
+    if (lens_to_air && ai >= asin(1.0 / n)) return false;   // total internal reflection
+    const double sgn = cos_ai > 0.0 ? 1.0 : (cos_ai < 0.0 ? -1.0 : 0.0);
+    const double cos_at = sgn * sqrt(1.0 - (a * a) * (1.0 - cos_ai * cos_ai));
+    const double at = acos(cos_at);
+    const double s1 = sin(ai - at) / sin(ai + at);
+    const double t1 = tan(ai - at) / tan(ai + at);
+    const double ra = u - 0.5 * (s1 * s1 + t1 * t1);
+    if (!(ra > 0.0)) return false;   // reflected, or NaN as at normal incidence
+    const double g = cos_at - a * cos_ai;
+    r.vx = a * r.vx + g * nx;
+    r.vy = a * r.vy + g * ny;
+    r.vz = a * r.vz + g * nz;
+    return true;
+}
+
+// the lens's spherical surface: intersection (:138-150) and normal (:200-210)
+__device__ __forceinline__ bool convex(Ray &r, double center, double rad, bool inward,
+                                       double half_outer, double n, double u) {
+    normalize(r);
+    const double pp = r.pz - center;
+    const double A = r.vx * r.vx + r.vy * r.vy + r.vz * r.vz;
+    const double B = 2.0 * (r.px * r.vx + r.py * r.vy + pp * r.vz);
+    const double C = r.px * r.px + r.py * r.py + pp * pp - rad * rad;
+    const double disc = sqrt(B * B - 4.0 * A * C);
+    const double t = inward ? (-B - disc) / (2.0 * A) : (-B + disc) / (2.0 * A);
+    r.px = r.px + r.vx * t;
+    r.py = r.py + r.vy * t;
+    r.pz = r.pz + r.vz * t;
+    if (!(radius(r) <= half_outer)) return false;
+    const double d = sqrt(rad * rad - (r.px * r.px + r.py * r.py));
+    const double dx = -r.px / d, dy = -r.py / d;
+    double nx = inward ? dx : -dx, ny = inward ? dy : -dy, nz = -1.0;
+    const double s = sqrt(nx * nx + ny * ny + nz * nz);
+    nx = nx / s;
+    ny = ny / s;
+    nz = nz / s;
+    // lens 1 (outward) leaves the glass here, lens 2 (inward) enters it
+    if (!refract(r, nx, ny, nz, n, !inward, u)) return false;
+    normalize(r);
+    return true;
+}
+
+// the lens's flat surface at z = pos, normal (0, 0, -1) (:103-113); the
+// first surface receives v already normalised in float32 (norm_first false)
+__device__ __forceinline__ bool plano(Ray &r, double pos, bool inward, double half_outer,
+                                      double n, double u, bool norm_first) {
+    if (norm_first) normalize(r);
+    hit_plane(r, pos);
+    if (!(radius(r) <= half_outer)) return false;
+    if (!refract(r, 0.0, 0.0, -1.0, n, inward, u)) return false;
+    normalize(r);
+    return true;
+}
+
+// annular slit: front and back faces (:79-84)
+__device__ __forceinline__ bool slit(Ray &r, double front, double back, double d_in,
+                                     double d_out) {
+    hit_plane(r, front);
+    double pp = radius(r);
+    if (!(pp < d_out && pp > d_in)) return false;
+    hit_plane(r, back);
+    pp = radius(r);
+    return pp < d_out && pp > d_in;
+}
+
+// laser-diode mount: photons pass where the mount is not (:336-376)
+__device__ __forceinline__ bool ld_mount(Ray &r, double front, double back, double a1,
+                                         double b1, double a2, double b2, double b3) {
+    hit_plane(r, front);
+    if (!(r.py > a1 * r.px + b1 || r.py < a2 * r.px + b2 || r.py < b3)) return false;
+    hit_plane(r, back);
+    return r.py > a1 * r.px + b1 || r.py < a2 * r.px + b2 || r.py < b3;
+}
+
+constexpr int kMaxZ = 4096;
+
+__global__ void __launch_bounds__(256) obd_kernel(pmo_obd_params prm, const float *__restrict__ p,
+                                                  const float *__restrict__ v,
+                                                  const float *__restrict__ w, int64_t n,
+                                                  double *__restrict__ intensity) {
+    extern __shared__ double s_int[];
+    for (int i = threadIdx.x; i < prm.n_z; i += blockDim.x) s_int[i] = 0.0;
+    __syncthreads();
+    const pmo::PhiloxKeys rk = pmo::philox_round_keys((uint32_t)prm.seed,
+                                                      (uint32_t)(prm.seed >> 32));
+    const double d_out = prm.slit_d / 2 + prm.slit_width / 2;
+    const double d_in = prm.slit_d / 2 - prm.slit_width / 2;
+    // mount edges: angle 68/180 rad, thickness 5, width 6 (:338-350)
+    const double ang = 68.0 / 180.0;
+    const double a1 = 1.0 / tan(ang) - 1.0 / (sin(ang) * cos(ang));
+    const double b1 = 6.0 / cos(ang);
+    const double a2 = (cos(ang) + 1.0) / sin(ang);
+    const double b2 = -6.0, b3 = -6.0;
+
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const float x0 = p[i], y0 = p[n + i];
+        // the first normalisation of v is in float32, like its input
+        const float vx0 = v[i], vy0 = v[n + i], vz0 = v[2 * n + i];
+        const float vs = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(vx0, vx0), __fmul_rn(vy0, vy0)),
+                                              __fmul_rn(vz0, vz0)));
+        const double ux = (double)__fdiv_rn(vx0, vs), uy = (double)__fdiv_rn(vy0, vs),
+                     uz = (double)__fdiv_rn(vz0, vs);
+        const double wi = (double)w[i];
+        for (int zi = 0; zi < prm.n_z; ++zi) {
+            const double Z = prm.z[zi];
+            // element positions of this Z (:454-470)
+            const double zl1 = -prm.bfl1 + Z;
+            const double zl2 = zl1 - prm.ct1 - prm.slit_thickness * 2 - prm.ct2 - prm.distance_2slits;
+            const double zs1 = zl1 - prm.ct1;
+            const double zs2 = zl2 + prm.ct2 + prm.slit_thickness;
+            const double zpd = zl2 - prm.bfl2 - prm.pd_correction;
+            Ray r;
+            r.px = prm.side ? (double)(float)((double)x0 - (Z + prm.side_dz) * prm.side_tan)
+                            : (double)x0;
+            r.py = (double)y0;
+            r.pz = 0.0;
+            r.vx = ux;
+            r.vy = uy;
+            r.vz = uz;
+            double u[4];
+            if (prm.fixed_u >= 0.0) {
+                u[0] = u[1] = u[2] = u[3] = prm.fixed_u;
+            } else {
+                const uint4 q = pmo::philox4x32_10(
+                    make_uint4((uint32_t)zi, 5u, (uint32_t)i, (uint32_t)((uint64_t)i >> 32)), rk);
+                u[0] = (double)q.x * 0x1p-32;
+                u[1] = (double)q.y * 0x1p-32;
+                u[2] = (double)q.z * 0x1p-32;
+                u[3] = (double)q.w * 0x1p-32;
+            }
+            // lens 1: flat face then curved face (:295-302)
+            if (!plano(r, zl1, false, prm.outer_d1 / 2, prm.n1, u[0], false)) continue;
+            if (!convex(r, zl1 - (prm.ct1 - prm.r1), prm.r1, false, prm.outer_d1 / 2, prm.n1,
+                        u[1]))
+                continue;
+            if (!slit(r, zs1, zs1 - prm.slit_thickness, d_in, d_out)) continue;
+            if (prm.ld_fix_part) {
+                const double zf = zs1 - prm.slit_thickness - 10;
+                if (!ld_mount(r, zf, zf - 5, a1, b1, a2, b2, b3)) continue;
+            }
+            if (!slit(r, zs2, zs2 - prm.slit_thickness, d_in, d_out)) continue;
+            // lens 2: curved face then flat face (:305-313)
+            if (!convex(r, zl2 + (prm.ct2 - prm.r2), prm.r2, true, prm.outer_d2 / 2, prm.n2,
+                        u[2]))
+                continue;
+            if (!plano(r, zl2, true, prm.outer_d2 / 2, prm.n2, u[3], true)) continue;
+            // photodiode (:325-334)
+            hit_plane(r, zpd);
+            if (radius(r) < prm.d_pd / 2) atomicAdd(s_int + zi, wi);
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < prm.n_z; i += blockDim.x)
+        if (s_int[i] != 0.0) atomicAdd(intensity + i, s_int[i]);
+}
+
+}  // namespace
+
+extern "C" {
+
+int pmo_run_obd(const pmo_obd_params *prm, const float *p, const float *v, const float *w, int64_t n,
+            double *intensity, void *stream) {
+    if (!prm || !intensity || n < 0 || (n > 0 && (!p || !v || !w))) return PMO_ERR_ARG;
+    if (!prm->z || prm->n_z < 1 || prm->n_z > kMaxZ) return PMO_ERR_ARG;
+    if (!(prm->fixed_u < 1.0)) return PMO_ERR_ARG;
+    if (n == 0) return PMO_OK;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    int sms = 148;
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess)
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int threads = 256;
+    int64_t blocks = (n + threads - 1) / threads;
+    if (blocks > (int64_t)sms * 8) blocks = (int64_t)sms * 8;
+    const size_t smem = (size_t)prm->n_z * sizeof(double);
+    if (smem > 48 * 1024 &&
+        cudaFuncSetAttribute(obd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess)
+        return PMO_ERR_CUDA;
+    obd_kernel<<<(unsigned)blocks, threads, smem, s>>>(*prm, p, v, w, n, intensity);
+    return cudaGetLastError() == cudaSuccess ? PMO_OK : PMO_ERR_CUDA;
+}
+
+}  // extern "C"

@@ -14,7 +14,8 @@ Usage::
 The reference imports pydicom, matplotlib and seaborn at module level although
 the transport path never calls them; they are stubbed with empty modules.
 The "turing" case runs the reference's CPU Turing-pattern generator
-(pymopt/modeling/_classes.py) on a small grid.
+(pymopt/modeling/_classes.py) on a small grid; the "obd" case runs its OBD
+ray tracing (pymopt/optics/_classes.py) on seeded synthetic exit photons.
 The fixtures are committed; nothing at test time needs the reference.
 """
 from __future__ import annotations
@@ -298,13 +299,78 @@ def run_turing_case(ref_root: str) -> str:
     return path
 
 
+def obd_photons(seed: int = 0, n: int = 50000):
+    """Seeded synthetic exit photons for the OBD stage: positions N(0, 1 mm)
+    in x and y, Lambertian directions leaving through the top (v_z < 0),
+    weights U[0.5, 1], plus 10 % going the other way; float32 like
+    get_result()."""
+    rng = np.random.default_rng(seed)
+    p = np.zeros((3, n), np.float32)
+    p[0], p[1] = rng.normal(0, 1.0, n), rng.normal(0, 1.0, n)
+    cos_t = np.sqrt(rng.random(n))
+    phi = 2 * np.pi * rng.random(n)
+    sin_t = np.sqrt(1 - cos_t ** 2)
+    v = np.stack([sin_t * np.cos(phi), sin_t * np.sin(phi), -cos_t]).astype(np.float32)
+    v[2, rng.random(n) < 0.1] *= -1
+    w = rng.uniform(0.5, 1.0, n).astype(np.float32)
+    return p, v, w
+
+
+def run_obd_case(ref_root: str) -> str:
+    """The reference's OBD ray tracing (pymopt/optics/_classes.py:381-566) on
+    seeded synthetic exit photons: OBD (with and without the LD fixing part)
+    and SideOBD, once with np.random.rand replaced by a constant 0.5 (every
+    Fresnel decision becomes R < 0.5, deterministic) and over ten seeds of
+    the real generator."""
+    _stub_modules()
+    sys.path.insert(0, ref_root)
+    from pymopt.optics import _classes as OC
+    OC.tqdm = lambda it: it
+    OC.calTime = lambda *a, **k: None
+    p, v, w = obd_photons()
+    out = {"n": int(w.size)}
+    real_rand = np.random.rand
+    with contextlib.redirect_stdout(io.StringIO()):
+        for name, cls, extra in (("obd", OC.OBD, {}),
+                                 ("obd_no_ld", OC.OBD, {"ld_fix_part": False}),
+                                 ("side", OC.SideOBD, {})):
+            runs = []
+            for mode in ["fixed"] + list(range(10)):
+                m = cls()
+                if extra:
+                    m.set_params(**extra)
+                m.set_monte_data(p=p.copy(), v=v.copy(), w=w.copy(), nPh=int(w.size))
+                if mode == "fixed":
+                    np.random.rand = lambda k: np.full(k, 0.5)
+                else:
+                    np.random.rand = real_rand
+                    np.random.seed(100 + mode)
+                try:
+                    z, inten = m.opticalAnalysisMeth()
+                finally:
+                    np.random.rand = real_rand
+                runs.append(inten)
+            out[name] = {"z": np.asarray(z).tolist(), "fixed": np.asarray(runs[0]).tolist(),
+                         "seeds": [np.asarray(r).tolist() for r in runs[1:]],
+                         "params": {k: (v_ if not isinstance(v_, np.generic) else v_.item())
+                                    for k, v_ in m.params.items()}}
+    out["generator"] = "tests/golden/make_golden.py (reference pymopt.optics, NumPy)"
+    path = os.path.join(HERE, "ref_obd.json")
+    with open(path, "w") as f:
+        json.dump(out, f)
+    return path
+
+
 def main():
     ref_root = sys.argv[1]
-    cases = sys.argv[2:] or list(PLATE_CASES) + ["c3", "volumes", "sources", "turing"]
+    cases = sys.argv[2:] or list(PLATE_CASES) + ["c3", "volumes", "sources", "turing", "obd"]
     for name in cases:
         t0 = time.time()
         if name == "turing":
             print("turing ->", run_turing_case(ref_root))
+            continue
+        if name == "obd":
+            print("obd ->", run_obd_case(ref_root))
             continue
         if name == "volumes":
             print("volumes ->", run_volumes_case(ref_root))

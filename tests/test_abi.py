@@ -80,7 +80,8 @@ def _c_offsets(struct_name, fields):
 @pytest.mark.parametrize("cls,name", [(A.PmoProblem, "pmo_problem"), (A.PmoTallies, "pmo_tallies"),
                                       (A.PmoLaunch, "pmo_launch"), (A.PmoGrad, "pmo_grad"),
                                       (A.PmoSlab, "pmo_slab"), (A.PmoBatchItem, "pmo_batch_item"),
-                                      (A.PmoBatch, "pmo_batch")])
+                                      (A.PmoBatch, "pmo_batch"),
+                                      (A.PmoObdParams, "pmo_obd_params")])
 def test_struct_layout_matches_header(cls, name):
     fields = [f[0] for f in cls._fields_]
     got = _c_offsets(name, fields)
