@@ -26,6 +26,13 @@
 // and counter (Z index, 5, photon_lo, photon_hi), as x * 2^-32 in [0, 1).
 // A fixed uniform (fixed_u in [0, 1)) replaces the draws for deterministic
 // comparisons.
+//
+// Work is ordered for speed without changing any decision:
+// - lens 1's flat face has a fixed normal, so its refraction and reflectance
+//   are computed once per photon rather than once per Z;
+// - the decisions do not change the ray, so the geometry is traced first;
+// - the reflectances (two acos, two sin, two tan each) and the draw are
+//   evaluated only for photons that reach the photodiode.
 #include "pmo_internal.h"
 
 namespace {
@@ -53,32 +60,50 @@ __device__ __forceinline__ double radius(const Ray &r) {
     return sqrt(r.px * r.px + r.py * r.py);
 }
 
-// refraction through a surface with unit normal nn, from air into glass of
-// index n or out of it, with the reference's Fresnel decision u - R > 0
-// (:152-188, :212-222); false: the photon is gone
+// Cosines of the incidence and transmission angles at one surface.
+struct Cosines {
+    double ai, at;
+};
+
+// Refraction through a surface with unit normal nn, from air into glass of
+// index n or out of it (:152-188): leaves the refracted direction, not yet
+// normalised, in r and returns the two cosines.  tir: the threshold
+// asin(1/n) when leaving the glass, where angles at or above it reflect
+// totally and the photon is gone (returns false).
 __device__ __forceinline__ bool refract(Ray &r, double nx, double ny, double nz, double n,
-                                        bool lens_to_air, double u) {
+                                        bool lens_to_air, double tir, Cosines &c) {
     const double cos_ai = nx * r.vx + ny * r.vy + nz * r.vz;
     const double a = lens_to_air ? n / 1.0 : 1.0 / n;
-    const double ai = acos(cos_ai);
-    if (lens_to_air && ai >= asin(1.0 / n)) return false;   // total internal reflection
+    if (lens_to_air && acos(cos_ai) >= tir) return false;   // total internal reflection
     const double sgn = cos_ai > 0.0 ? 1.0 : (cos_ai < 0.0 ? -1.0 : 0.0);
     const double cos_at = sgn * sqrt(1.0 - (a * a) * (1.0 - cos_ai * cos_ai));
-    const double at = acos(cos_at);
-    const double s1 = sin(ai - at) / sin(ai + at);
-    const double t1 = tan(ai - at) / tan(ai + at);
-    const double ra = u - 0.5 * (s1 * s1 + t1 * t1);
-    if (!(ra > 0.0)) return false;   // reflected, or NaN as at normal incidence
     const double g = cos_at - a * cos_ai;
     r.vx = a * r.vx + g * nx;
     r.vy = a * r.vy + g * ny;
     r.vz = a * r.vz + g * nz;
+    c.ai = cos_ai;
+    c.at = cos_at;
     return true;
 }
 
-// the lens's spherical surface: intersection (:138-150) and normal (:200-210)
+// Fresnel reflectance of the reference, 0.5 [(sin(ai-at)/sin(ai+at))^2 +
+// (tan(ai-at)/tan(ai+at))^2] (:212-215); NaN at normal incidence.  It does
+// not change the ray, so the kernel evaluates it only for photons that reach
+// the photodiode.
+__device__ __forceinline__ double reflectance(const Cosines &c) {
+    const double ai = acos(c.ai), at = acos(c.at);
+    const double s1 = sin(ai - at) / sin(ai + at);
+    const double t1 = tan(ai - at) / tan(ai + at);
+    return 0.5 * (s1 * s1 + t1 * t1);
+}
+
+// the reference's decision rand - R > 0 (false for NaN R)
+__device__ __forceinline__ bool passes(double u, double R) { return u - R > 0.0; }
+
+// the lens's spherical surface: intersection (:138-150), normal (:200-210)
+// and refraction; the cosines go to c for the deferred Fresnel decision
 __device__ __forceinline__ bool convex(Ray &r, double center, double rad, bool inward,
-                                       double half_outer, double n, double u) {
+                                       double half_outer, double n, double tir, Cosines &c) {
     normalize(r);
     const double pp = r.pz - center;
     const double A = r.vx * r.vx + r.vy * r.vy + r.vz * r.vz;
@@ -98,19 +123,19 @@ __device__ __forceinline__ bool convex(Ray &r, double center, double rad, bool i
     ny = ny / s;
     nz = nz / s;
     // lens 1 (outward) leaves the glass here, lens 2 (inward) enters it
-    if (!refract(r, nx, ny, nz, n, !inward, u)) return false;
+    if (!refract(r, nx, ny, nz, n, !inward, tir, c)) return false;
     normalize(r);
     return true;
 }
 
-// the lens's flat surface at z = pos, normal (0, 0, -1) (:103-113); the
-// first surface receives v already normalised in float32 (norm_first false)
-__device__ __forceinline__ bool plano(Ray &r, double pos, bool inward, double half_outer,
-                                      double n, double u, bool norm_first) {
-    if (norm_first) normalize(r);
+// lens 2's flat face at z = pos, normal (0, 0, -1), leaving the glass
+// (:103-113)
+__device__ __forceinline__ bool plano_out(Ray &r, double pos, double half_outer, double n,
+                                          double tir, Cosines &c) {
+    normalize(r);
     hit_plane(r, pos);
     if (!(radius(r) <= half_outer)) return false;
-    if (!refract(r, 0.0, 0.0, -1.0, n, inward, u)) return false;
+    if (!refract(r, 0.0, 0.0, -1.0, n, true, tir, c)) return false;
     normalize(r);
     return true;
 }
@@ -137,7 +162,7 @@ __device__ __forceinline__ bool ld_mount(Ray &r, double front, double back, doub
 
 constexpr int kMaxZ = 4096;
 
-__global__ void __launch_bounds__(256) obd_kernel(pmo_obd_params prm, const float *__restrict__ p,
+__global__ void __launch_bounds__(256, 4) obd_kernel(pmo_obd_params prm, const float *__restrict__ p,
                                                   const float *__restrict__ v,
                                                   const float *__restrict__ w, int64_t n,
                                                   double *__restrict__ intensity) {
@@ -154,6 +179,9 @@ __global__ void __launch_bounds__(256) obd_kernel(pmo_obd_params prm, const floa
     const double b1 = 6.0 / cos(ang);
     const double a2 = (cos(ang) + 1.0) / sin(ang);
     const double b2 = -6.0, b3 = -6.0;
+    // total-internal-reflection thresholds asin(nt / ni) of the glass-to-air
+    // surfaces (:176)
+    const double tir1 = asin(1.0 / prm.n1), tir2 = asin(1.0 / prm.n2);
 
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
@@ -165,6 +193,19 @@ __global__ void __launch_bounds__(256) obd_kernel(pmo_obd_params prm, const floa
         const double ux = (double)__fdiv_rn(vx0, vs), uy = (double)__fdiv_rn(vy0, vs),
                      uz = (double)__fdiv_rn(vz0, vs);
         const double wi = (double)w[i];
+        // Lens 1's flat face has the fixed normal (0, 0, -1): the incidence
+        // angle, the reflectance and the refracted direction do not depend on
+        // Z, only the hit point and the draw do.  Computed once per photon,
+        // with the same operations as inside the scan.
+        Ray r1;
+        r1.px = r1.py = r1.pz = 0.0;
+        r1.vx = ux;
+        r1.vy = uy;
+        r1.vz = uz;
+        Cosines c1;
+        refract(r1, 0.0, 0.0, -1.0, prm.n1, false, 0.0, c1);
+        const double R1 = reflectance(c1);
+        normalize(r1);
         for (int zi = 0; zi < prm.n_z; ++zi) {
             const double Z = prm.z[zi];
             // element positions of this Z (:454-470)
@@ -181,6 +222,33 @@ __global__ void __launch_bounds__(256) obd_kernel(pmo_obd_params prm, const floa
             r.vx = ux;
             r.vy = uy;
             r.vz = uz;
+            // lens 1: flat face (the float32-normalised v goes in as it is)
+            // then curved face (:295-302)
+            hit_plane(r, zl1);
+            if (!(radius(r) <= prm.outer_d1 / 2)) continue;
+            r.vx = r1.vx;
+            r.vy = r1.vy;
+            r.vz = r1.vz;
+            Cosines c2, c3, c4;
+            if (!convex(r, zl1 - (prm.ct1 - prm.r1), prm.r1, false, prm.outer_d1 / 2, prm.n1,
+                        tir1, c2))
+                continue;
+            if (!slit(r, zs1, zs1 - prm.slit_thickness, d_in, d_out)) continue;
+            if (prm.ld_fix_part) {
+                const double zf = zs1 - prm.slit_thickness - 10;
+                if (!ld_mount(r, zf, zf - 5, a1, b1, a2, b2, b3)) continue;
+            }
+            if (!slit(r, zs2, zs2 - prm.slit_thickness, d_in, d_out)) continue;
+            // lens 2: curved face then flat face (:305-313)
+            if (!convex(r, zl2 + (prm.ct2 - prm.r2), prm.r2, true, prm.outer_d2 / 2, prm.n2,
+                        0.0, c3))
+                continue;
+            if (!plano_out(r, zl2, prm.outer_d2 / 2, prm.n2, tir2, c4)) continue;
+            // photodiode (:325-334)
+            hit_plane(r, zpd);
+            if (!(radius(r) < prm.d_pd / 2)) continue;
+            // the four Fresnel decisions, which do not change the ray: drawn
+            // and taken only for photons that reach the photodiode
             double u[4];
             if (prm.fixed_u >= 0.0) {
                 u[0] = u[1] = u[2] = u[3] = prm.fixed_u;
@@ -192,25 +260,10 @@ __global__ void __launch_bounds__(256) obd_kernel(pmo_obd_params prm, const floa
                 u[2] = (double)q.z * 0x1p-32;
                 u[3] = (double)q.w * 0x1p-32;
             }
-            // lens 1: flat face then curved face (:295-302)
-            if (!plano(r, zl1, false, prm.outer_d1 / 2, prm.n1, u[0], false)) continue;
-            if (!convex(r, zl1 - (prm.ct1 - prm.r1), prm.r1, false, prm.outer_d1 / 2, prm.n1,
-                        u[1]))
+            if (!passes(u[0], R1) || !passes(u[1], reflectance(c2)) ||
+                !passes(u[2], reflectance(c3)) || !passes(u[3], reflectance(c4)))
                 continue;
-            if (!slit(r, zs1, zs1 - prm.slit_thickness, d_in, d_out)) continue;
-            if (prm.ld_fix_part) {
-                const double zf = zs1 - prm.slit_thickness - 10;
-                if (!ld_mount(r, zf, zf - 5, a1, b1, a2, b2, b3)) continue;
-            }
-            if (!slit(r, zs2, zs2 - prm.slit_thickness, d_in, d_out)) continue;
-            // lens 2: curved face then flat face (:305-313)
-            if (!convex(r, zl2 + (prm.ct2 - prm.r2), prm.r2, true, prm.outer_d2 / 2, prm.n2,
-                        u[2]))
-                continue;
-            if (!plano(r, zl2, true, prm.outer_d2 / 2, prm.n2, u[3], true)) continue;
-            // photodiode (:325-334)
-            hit_plane(r, zpd);
-            if (radius(r) < prm.d_pd / 2) atomicAdd(s_int + zi, wi);
+            atomicAdd(s_int + zi, wi);
         }
     }
     __syncthreads();

@@ -207,3 +207,34 @@ class TuringPattern:
         if self.tile_num_xz != 0:
             vol = np.tile(vol, (self.tile_num_xz, self.tile_num_y, self.tile_num_xz))
         return vol
+
+
+def main(argv=None) -> int:
+    """``python -m pymonteopt_b200.turing``: time TuringPattern.modeling at
+    the reference's default size (520^3, 100 steps) and print one JSON line."""
+    import argparse
+    import tempfile
+    import time
+    ap = argparse.ArgumentParser(description=main.__doc__.split("\n")[0])
+    ap.add_argument("--grid", type=int, default=40)
+    ap.add_argument("--length", type=int, default=13)
+    ap.add_argument("--repetition", type=int, default=100)
+    args = ap.parse_args(argv)
+    tp = TuringPattern()
+    tp.set_params(grid=args.grid, dx=1 / args.grid, length=args.length,
+                  repetition=args.repetition, seed=1)
+    with tempfile.TemporaryDirectory() as d:
+        tp.modeling(d)                                   # warm-up (cuFFT plans)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        vol = tp.modeling(d)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+    print(json.dumps({"gridsize": tp.gridsize, "repetition": tp.repetition, "seconds": dt,
+                      "steps_per_s": tp.repetition / dt, "bv_tv_real": tp.bv_tv_real,
+                      "volume_shape": list(vol.shape)}))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
