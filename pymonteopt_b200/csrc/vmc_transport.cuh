@@ -163,6 +163,17 @@ enum : int { kChunk = 64 };
 #endif
 constexpr int kCrossPerIter = PMO_CROSS_PER_ITER;
 
+// Face crossings are rare next to interactions, so a warp that runs the
+// crossing code for one or two lanes spends a full warp instruction per lane
+// used.  A lane that needs a crossing therefore waits, its state untouched,
+// until at least this many lanes of its warp (or a quarter of the active
+// lanes, or all of them) need one; the crossing code then runs for all of
+// them at once.  Photon histories do not depend on it.
+#ifndef PMO_CROSS_BATCH
+#define PMO_CROSS_BATCH 8
+#endif
+constexpr int kCrossBatch = PMO_CROSS_BATCH;
+
 // GRAD: the gradient replay (pmo_run_grad).  It replays the photons whose
 // forward score record gives q = coef[bin] * w != 0 along the same path (same
 // arithmetic, same Philox draws) and accumulates -q*L and q*(n/mu_s - L) per
@@ -593,7 +604,8 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
     // One interaction cycle of the photon in flight: draw a step, cross voxel
     // faces until the step is spent, then absorb, roulette and scatter.
     // Returns true while the photon stays in flight.
-    auto cycle = [&]() -> bool {
+    // act: the warp's lanes with a photon in flight (all of them call cycle)
+    auto cycle = [&](unsigned act) -> bool {
         if (!pending) {
             const uint4 rn =
                 philox4x32_10(make_uint4(k, 0u, (uint32_t)pid, (uint32_t)(pid >> 32)), kp.rk);
@@ -605,6 +617,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             pending = true;
         }
         int budget = kCrossPerIter;
+        bool first = true;
         for (;;) {
             // distance to the nearest face; db starts at 1000 (:80-90)
             const R ax_ = xsub(copysign(hwl, vx), px);
@@ -619,7 +632,15 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             if (dy < db) { db = dy; ax = 1; }
             if (dz < db) { db = dz; ax = 2; }
             const R dbmt = xmul(db, mt);
-            if (!(st >= dbmt)) {
+            const bool hop = !(st >= dbmt);
+            if (kCrossBatch > 1 && first) {
+                first = false;
+                const unsigned xm = __ballot_sync(act, !hop);
+                const int nx = __popc(xm), na = __popc(act);
+                const bool go = nx >= kCrossBatch || 4 * nx >= na || nx == na;
+                if (!hop && !go) return true;   // wait; the draws and st are kept
+            }
+            if (hop) {
                 // hop inside the voxel or box (:170-175)
                 const R s = xmul(st, imt);
                 px = xfma(vx, s, px);
@@ -849,7 +870,8 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             need &= ~taken;
         }
         if (!__any_sync(FULL, active || more)) break;
-        if (active) active = cycle();
+        const unsigned act = __ballot_sync(FULL, active);
+        if (active) active = cycle(act);
     }
 
     // ---- block epilogue: reduce thread totals, flush privatised tallies ----
