@@ -152,16 +152,23 @@ struct SmemLayout {
 
 enum : int { kChunk = 64 };
 
-// A pass of the warp loop does, per lane, either one face crossing or one
-// hop and interaction; a lane that crosses continues its step next pass.  A
-// warp runs a code path until its slowest lane is done, so letting a lane
-// cross several faces in a pass keeps the others idle (measured on C2, one
-// B200: 1 crossing per pass 1.30e8 photons/s, 2 -> 0.90e8, unlimited ->
-// 0.80e8).  The photon's sequence of operations does not depend on this.
+// Face crossings a lane may process per pass of the warp loop before it
+// yields.  A warp executes the crossing loop until its slowest lane is done;
+// capping it keeps lanes that are ready to interact from idling behind one
+// lane that crosses many faces.  The photon's sequence of operations, and so
+// its result, does not depend on this value.  Measured on C2 (one B200):
+// 1 -> 1.30e8 photons/s, 2 -> 0.90e8, 4 -> 0.82e8, unlimited -> 0.80e8.
+// With uniform boxes a lane that crossed yields at once, so the interaction
+// code runs once per pass; with voxel-by-voxel stepping, where crossings are
+// as frequent as interactions, it goes on to hop in the same pass.
+#ifndef PMO_CROSS_PER_ITER
+#define PMO_CROSS_PER_ITER 1
+#endif
+constexpr int kCrossPerIter = PMO_CROSS_PER_ITER;
 
-// Face crossings are rare next to interactions, so a warp that runs the
-// crossing code for one or two lanes spends a full warp instruction per lane
-// used.  A lane that needs a crossing therefore waits, its state untouched,
+// With uniform boxes, face crossings are rare next to interactions, so a warp
+// that runs the crossing code for one or two lanes spends a full warp
+// instruction per lane used.  A lane that needs a crossing therefore waits, its state untouched,
 // until at least this many lanes of its warp (or a quarter of the active
 // lanes, or all of them) need one; the crossing code then runs for all of
 // them at once.  Photon histories do not depend on it.
@@ -597,10 +604,15 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
         return true;
     };
 
-    // One pass for the photon in flight: draw a step if none is pending, then
-    // either cross one box face (the step goes on next pass) or hop, absorb,
-    // roulette and scatter.  Returns true while the photon stays in flight.
-    // act: the warp's lanes with a photon in flight (all of them call cycle)
+    // One interaction cycle of the photon in flight: draw a step, cross voxel
+    // faces until the step is spent, then absorb, roulette and scatter.
+    // Returns true while the photon stays in flight.
+    // act: the warp's lanes with a photon in flight (all of them call cycle).
+    // Box stepping batches crossings and yields after one; voxel stepping,
+    // whose crossings are frequent, does neither (measured: each costs it
+    // 3-16 %).
+    constexpr int kBatch = SKIP ? kCrossBatch : 1;
+    constexpr bool kYield = SKIP;
     auto cycle = [&](unsigned act) -> bool {
         if (!pending) {
             const uint4 rn =
@@ -612,27 +624,41 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             rw = rn.w;
             pending = true;
         }
-        // distance to the nearest face; db starts at 1000 (:80-90)
-        const R ax_ = xsub(copysign(hwl, vx), px);
-        const R ay_ = xsub(copysign(hwl, vy), py);
-        const R az_ = xsub(copysign(hwz, vz), pz);
-        const R dx = kInv ? xmul(ax_, ivx) : xdiv(ax_, vx);
-        const R dy = kInv ? xmul(ay_, ivy) : xdiv(ay_, vy);
-        const R dz = kInv ? xmul(az_, ivz) : xdiv(az_, vz);
-        R db = R(1000);
-        int ax = 0;
-        if (dx < db) { db = dx; ax = 0; }
-        if (dy < db) { db = dy; ax = 1; }
-        if (dz < db) { db = dz; ax = 2; }
-        const R dbmt = xmul(db, mt);
-        const bool hop = !(st >= dbmt);
-        if (kCrossBatch > 1) {
-            const unsigned xm = __ballot_sync(act, !hop);
-            const int nx = __popc(xm), na = __popc(act);
-            const bool go = nx >= kCrossBatch || 4 * nx >= na || nx == na;
-            if (!hop && !go) return true;   // wait; the draws and st are kept
-        }
-        if (!hop) {
+        int budget = kCrossPerIter;
+        bool first = true;
+        for (;;) {
+            // distance to the nearest face; db starts at 1000 (:80-90)
+            const R ax_ = xsub(copysign(hwl, vx), px);
+            const R ay_ = xsub(copysign(hwl, vy), py);
+            const R az_ = xsub(copysign(hwz, vz), pz);
+            const R dx = kInv ? xmul(ax_, ivx) : xdiv(ax_, vx);
+            const R dy = kInv ? xmul(ay_, ivy) : xdiv(ay_, vy);
+            const R dz = kInv ? xmul(az_, ivz) : xdiv(az_, vz);
+            R db = R(1000);
+            int ax = 0;
+            if (dx < db) { db = dx; ax = 0; }
+            if (dy < db) { db = dy; ax = 1; }
+            if (dz < db) { db = dz; ax = 2; }
+            const R dbmt = xmul(db, mt);
+            const bool hop = !(st >= dbmt);
+            if (kBatch > 1 && first) {
+                first = false;
+                const unsigned xm = __ballot_sync(act, !hop);
+                const int nx = __popc(xm), na = __popc(act);
+                const bool go = nx >= kCrossBatch || 4 * nx >= na || nx == na;
+                if (!hop && !go) return true;   // wait; the draws and st are kept
+            }
+            if (hop) {
+                // hop inside the voxel or box (:170-175)
+                const R s = xmul(st, imt);
+                px = xfma(vx, s, px);
+                py = xfma(vy, s, py);
+                pz = xfma(vz, s, pz);
+                if (GRAD) gL += (float)s;
+                break;
+            }
+            if (budget == 0) return true;  // yield; this crossing comes next pass
+            --budget;
             // move to the face and snap (:92-96)
             px = xfma(vx, db, px);
             py = xfma(vy, db, py);
@@ -700,7 +726,8 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             if (PROPS == PMO_PROPS_LABEL && nlab == lab) {
                 // same label on the other side: same n and mu (:154-167)
                 enter();
-                return true;   // the step goes on next pass
+                if (kYield) return true;   // the step goes on next pass
+                continue;
             }
             if (nlab != kp.end_label && !s_valid[nlab]) { fail(PMO_C_ERR_LABEL); return false; }
             const R nt = s_tab[nlab].n;
@@ -742,7 +769,8 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
                     else if (ax == 1) { vy = -vy; ivy = -ivy; }
                     else { vz = -vz; ivz = -ivz; }
                     atomicAdd(s_cnt + PMO_C_REFLECT, 1ull);
-                    return true;
+                    if (kYield) return true;
+                    continue;
                 }
                 // refract: tangential * ni/nt, normal = sign * cos(at) (:124-134)
                 vx = ax == 0 ? xmul(sgn(vx), cb) : xmul(vx, nr);
@@ -762,15 +790,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
                 return false;
             }
             load_props();
-            return true;   // the step goes on next pass
-        }
-        // hop inside the voxel or box (:170-175)
-        {
-            const R s = xmul(st, imt);
-            px = xfma(vx, s, px);
-            py = xfma(vy, s, py);
-            pz = xfma(vz, s, pz);
-            if (GRAD) gL += (float)s;
+            if (kYield) return true;
         }
 
         pending = false;
