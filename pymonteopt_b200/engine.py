@@ -285,3 +285,51 @@ def cuvmc(add: torch.Tensor, p: torch.Tensor, v: torch.Tensor, w: torch.Tensor,
                        C.c_void_p(workspace.data_ptr()), workspace.numel(),
                        _stream_handle(stream))
     check(st, "pmo_cuvmc")
+
+
+def main(argv=None) -> int:
+    """``python -m pymonteopt_b200.engine``: time plain launches on one of the
+    synthetic volumes and print one JSON line (photons/s of the best launch)."""
+    import argparse
+    import json
+    from . import volumes as V
+    vols = {"c1": V.c1_slab, "c2": V.c2_skin, "c3": V.c3_ct_like, "c4": V.c4_voxel_props}
+    flu = {"none": A.PMO_FLU_NONE, "global": A.PMO_FLU_GLOBAL}
+    ap = argparse.ArgumentParser(description=main.__doc__.split("\n")[0])
+    ap.add_argument("--volume", choices=sorted(vols), default="c3")
+    ap.add_argument("--photons", type=float, default=1e7)
+    ap.add_argument("--fluence", choices=sorted(flu), default="none")
+    ap.add_argument("--nr", type=int, default=100)
+    ap.add_argument("--dr", type=float, default=0.1)
+    ap.add_argument("--reps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=1)
+    ap.add_argument("--block-threads", type=int, default=0)
+    args = ap.parse_args(argv)
+    n = int(args.photons)
+    dp = DeviceProblem(vols[args.volume]())
+    spec = TallySpec(nr=args.nr, dr=args.dr, fluence=flu[args.fluence])
+    tallies = Tallies(dp, spec, n)
+    best = float("inf")
+    for r in range(args.warmup + args.reps):
+        tallies.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        run_plain(dp, n, 1 + r, tallies=tallies, block_threads=args.block_threads)
+        e1.record()
+        torch.cuda.synchronize()
+        tallies.check()
+        if r >= args.warmup:
+            best = min(best, e0.elapsed_time(e1) / 1e3)
+    s = tallies.summary()
+    c = s["counters"]
+    print(json.dumps({"volume": args.volume, "photons": n, "fluence": args.fluence,
+                      "seconds": best, "photons_per_s": n / best,
+                      "Rd": float(s["Rd"]), "Tt": float(s["Tt"]), "A": float(s["A"]),
+                      "interactions_per_photon": float(c[A.PMO_C_INTERACT]) / n,
+                      "crossings_per_photon": float(c[A.PMO_C_CROSS]) / n,
+                      "fresnel_per_photon": float(c[A.PMO_C_FRESNEL]) / n}))
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
