@@ -34,10 +34,11 @@ static inline void pmo_philox4x32_10(const uint32_t ctr_in[4],
     out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
 }
 
-/* 32-bit word -> uniform in (0, 1]: ((x >> 8) + 1) * 2^-24.  Every value is
-   exact in float and double, so FP32 and FP64 builds see identical draws. */
+/* 32-bit word -> uniform in (0, 1]: 1 - (x >> 9) * 2^-23, the value the
+   device forms as 2 - f from the float f = 1 + (x >> 9) * 2^-23.  Every value
+   is exact in float and double, so FP32 and FP64 builds see identical draws. */
 static inline double pmo_u01(uint32_t x) {
-    return (double)((x >> 8) + 1u) * (1.0 / 16777216.0);
+    return 1.0 - (double)(x >> 9) * (1.0 / 8388608.0);
 }
 
 #endif

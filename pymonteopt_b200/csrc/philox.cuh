@@ -52,11 +52,14 @@ __device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
     return c;
 }
 
-// 32-bit word -> uniform in (0, 1]: ((x >> 8) + 1) * 2^-24, exact in float
-// and in double, so the FP32 and FP64 builds consume identical draws.
+// 32-bit word -> uniform in (0, 1]: 2 - f with f = 1 + (x >> 9) * 2^-23 the
+// float whose mantissa is the word's top 23 bits, i.e. 1 - (x >> 9) * 2^-23.
+// Every value is exact in float and in double, so the FP32 and FP64 builds
+// consume identical draws; a bit merge and one subtraction replace an
+// integer-to-float conversion and a multiply.
 template <typename R>
 __device__ __forceinline__ R u01(uint32_t x) {
-    return (R)((x >> 8) + 1u) * (R)5.9604644775390625e-8;
+    return (R)2 - (R)__uint_as_float((x >> 9) | 0x3f800000u);
 }
 
 }  // namespace pmo

@@ -634,11 +634,10 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             const R dx = kInv ? xmul(ax_, ivx) : xdiv(ax_, vx);
             const R dy = kInv ? xmul(ay_, ivy) : xdiv(ay_, vy);
             const R dz = kInv ? xmul(az_, ivz) : xdiv(az_, vz);
-            R db = R(1000);
-            int ax = 0;
-            if (dx < db) { db = dx; ax = 0; }
-            if (dy < db) { db = dy; ax = 1; }
-            if (dz < db) { db = dz; ax = 2; }
+            // min without the axis (a NaN distance, 0/0 on a face the photon
+            // runs along, is skipped as by the reference's comparisons); the
+            // axis is only needed for a crossing and is found there
+            const R db = fmin(fmin(fmin(R(1000), dx), dy), dz);
             const R dbmt = xmul(db, mt);
             const bool hop = !(st >= dbmt);
             if (kBatch > 1 && first) {
@@ -659,6 +658,9 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             }
             if (budget == 0) return true;  // yield; this crossing comes next pass
             --budget;
+            // the first axis at the minimum, the reference's strict-less scan
+            // from x to z (a tie goes to the lower axis)
+            const int ax = dx == db ? 0 : (dy == db ? 1 : (dz == db ? 2 : 0));
             // move to the face and snap (:92-96)
             px = xfma(vx, db, px);
             py = xfma(vy, db, py);

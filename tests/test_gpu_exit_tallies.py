@@ -28,6 +28,23 @@ def _model(**kw):
     return m
 
 
+def _edge_slack(v, w, nn, n):
+    """Per-bin weight (in the histogram's units) of the exits whose angle lies
+    within 1e-5 bin widths of a bin edge.  The device takes arccos and divides
+    by the bin width in single precision (error below 4e-6 bin widths), the
+    host in double, so such an exit may be counted one bin over."""
+    da = np.pi / (2 * nn)
+    t = np.arccos(np.abs(np.asarray(v[2], np.float64))) / da
+    e = np.rint(t).astype(np.int64)
+    amb = np.abs(t - e) < 1e-5
+    slack = np.zeros(nn)
+    for side in (e[amb] - 1, e[amb]):
+        ok = (side >= 0) & (side < nn)
+        np.add.at(slack, side[ok], np.asarray(w, np.float64)[amb][ok])
+    alpha = (np.arange(nn) + 0.5) * da
+    return slack / (4 * np.pi * np.sin(alpha) * np.sin(da / 2) * n)
+
+
 @pytest.mark.parametrize("precision", ["fp32", "fp64"])
 def test_angle_resolved_matches_host_scoring(cuda, precision):
     m = _model(precision=precision).start(rand_seed=9)
@@ -38,7 +55,11 @@ def test_angle_resolved_matches_host_scoring(cuda, precision):
         a_host, host = metrics.angularyResolved(v[:, sel], w[sel], m.n_ang, n)
         np.testing.assert_allclose(a_dev, a_host, rtol=0, atol=1e-12)
         assert host.sum() > 0
-        np.testing.assert_allclose(dev, host, rtol=1e-4, atol=1e-6 * host.max())
+        slack = _edge_slack(v[:, sel], w[sel], m.n_ang, n)
+        assert np.all(np.abs(dev - host) <= 1e-4 * np.abs(host) + slack + 1e-9 * host.max()), \
+            (np.abs(dev - host), slack)
+        # only a handful of exits lie that close to an edge
+        assert slack.sum() < 1e-3 * host.sum()
 
 
 def test_line_profile_matches_host_scoring(cuda):

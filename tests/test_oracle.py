@@ -150,6 +150,6 @@ def test_philox_oracle_structure():
     flips = np.unpackbits((a ^ k2).view(np.uint8)).reshape(512, -1).sum(1)
     assert 50 < flips.mean() < 78
     # uniforms in (0, 1]
-    u = ((a.astype(np.uint64) >> 8) + 1) / 2.0 ** 24
+    u = 1.0 - (a.astype(np.uint64) >> 9) / 2.0 ** 23
     assert u.min() > 0 and u.max() <= 1
     assert abs(u.mean() - 0.5) < 0.01
