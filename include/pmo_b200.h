@@ -322,6 +322,15 @@ typedef struct pmo_batch_item {
 #define PMO_BR_BALANCE   7        /* energy ledger residual / launched weight  */
 #define PMO_BR_N         8
 
+/* pmo_batch.tally_mode.  PMO_BT_THREAD: each thread keeps the sums of the
+   problem it works on in shared memory and adds them to global memory when
+   it moves to another problem (few global atomics; shared memory of
+   threads * 13 doubles).  PMO_BT_GLOBAL: every sum goes straight to global
+   memory with an atomic (no shared memory; atomics on the same few addresses
+   for photons of one problem). */
+#define PMO_BT_THREAD 0
+#define PMO_BT_GLOBAL 1
+
 typedef struct pmo_batch {
     const pmo_slab *slabs;        /* device array of n_problems */
     int32_t n_problems;
@@ -338,6 +347,8 @@ typedef struct pmo_batch {
                                      global timer) or NULL */
     int32_t precision;            /* PMO_FP32 or PMO_FP64 */
     uint32_t max_events;          /* 0 = 2^26 */
+    int32_t tally_mode;           /* where per-problem sums gather:
+                                     PMO_BT_THREAD or PMO_BT_GLOBAL */
 } pmo_batch;
 
 /*

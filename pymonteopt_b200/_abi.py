@@ -172,6 +172,7 @@ class PmoGrad(C.Structure):
 PMO_BS_RD, PMO_BS_RD_L, PMO_BS_RD_N, PMO_BS_TT, PMO_BS_TT_L, PMO_BS_TT_N = 0, 1, 2, 3, 4, 5
 PMO_BS_ABS, PMO_BS_WINIT, PMO_BS_RGAIN, PMO_BS_RLOSS, PMO_BS_ERRW, PMO_BS_INTER = 6, 7, 8, 9, 10, 11
 PMO_BS_N = 16
+PMO_BT_THREAD, PMO_BT_GLOBAL = 0, 1
 PMO_BR_RD, PMO_BR_TT, PMO_BR_A = 0, 1, 2
 PMO_BR_DRD_DMA, PMO_BR_DRD_DMS, PMO_BR_DTT_DMA, PMO_BR_DTT_DMS = 3, 4, 5, 6
 PMO_BR_BALANCE = 7
@@ -196,6 +197,7 @@ class PmoBatch(C.Structure):
         ("sums", C.c_void_p), ("bins", C.c_void_p),
         ("remaining", C.c_void_p), ("t_done", C.c_void_p),
         ("precision", C.c_int32), ("max_events", C.c_uint32),
+        ("tally_mode", C.c_int32),
     ]
 
 

@@ -9,9 +9,11 @@ Monte Carlo derivatives with respect to mu_a and mu_s.  The launch sequence
 (clearing the sums, the kernel, the FP64 finalisation) is captured in a CUDA
 graph and replayed.
 
-The launch shape (threads per block, photons per work item) is chosen by a
-small autotuner that times candidate shapes on a down-scaled copy of the
-batch and caches the winner per device and batch signature.
+The launch shape (threads per block, photons per work item) and where the
+per-problem sums gather (privatised per thread in shared memory, or straight
+to global memory) are chosen by a small autotuner. It times candidates on a
+down-scaled copy of the batch and caches the winner per device and batch
+signature.
 """
 from __future__ import annotations
 
@@ -61,7 +63,8 @@ class SlabBatch:
 
     def __init__(self, ma, ms, g, n, thickness, photons, *, n_ambient=1.0, nr: int = 32,
                  dr=0.1, seed: int = 0, precision: int = A.PMO_FP32, device=None,
-                 block_threads: int = 0, chunk: int = 0, autotune: bool = True):
+                 block_threads: int = 0, chunk: int = 0, tally_mode: Optional[int] = None,
+                 autotune: bool = True):
         load()
         self.device = E.require_cuda(device)
         P = len(ma)
@@ -93,9 +96,13 @@ class SlabBatch:
         self.workspace = torch.zeros(int(load().pmo_workspace_bytes()), dtype=torch.uint8,
                                      device=dev)
         self.graph = None
-        if autotune and not (block_threads and chunk):
-            block_threads, chunk = self.autotune()
+        if tally_mode not in (None, A.PMO_BT_THREAD, A.PMO_BT_GLOBAL):
+            raise ValueError("tally_mode must be PMO_BT_THREAD or PMO_BT_GLOBAL")
+        if autotune and not (block_threads and chunk and tally_mode is not None):
+            block_threads, chunk, tally_mode = self.autotune(
+                block_threads=block_threads, chunk=chunk, tally_mode=tally_mode)
         self.block_threads = block_threads or 128
+        self.tally_mode = A.PMO_BT_THREAD if tally_mode is None else int(tally_mode)
         self.set_chunk(chunk or 256)
 
     # ------------------------------------------------------------------
@@ -107,7 +114,7 @@ class SlabBatch:
         self.graph = None
 
     def _struct(self, slabs=None, items=None, n_items=None, sums=None, bins=None,
-                remaining=None, t_done=None, P=None) -> A.PmoBatch:
+                remaining=None, t_done=None, P=None, tally_mode=None) -> A.PmoBatch:
         b = A.PmoBatch()
         b.slabs = (slabs if slabs is not None else self.slabs).data_ptr()
         b.n_problems = P or self.P
@@ -120,6 +127,7 @@ class SlabBatch:
         b.remaining = (remaining if remaining is not None else self.remaining).data_ptr()
         b.t_done = (t_done if t_done is not None else self.t_done).data_ptr()
         b.precision = self.precision
+        b.tally_mode = self.tally_mode if tally_mode is None else int(tally_mode)
         return b
 
     def launch(self, stream=None) -> None:
@@ -180,30 +188,46 @@ class SlabBatch:
         }
 
     # ------------------------------------------------------------------
-    def autotune(self, candidates=None, scale: float = 1 / 64) -> tuple:
-        """Pick (threads per block, photons per work item) by timing each
-        candidate on the batch with every budget scaled by ``scale``."""
+    def autotune(self, candidates=None, scale: float = 1 / 64, mode_scale: float = 1 / 8,
+                 block_threads: int = 0, chunk: int = 0,
+                 tally_mode: Optional[int] = None) -> tuple:
+        """Pick (threads per block, photons per work item, tally mode).
+
+        The shapes are timed with per-thread privatised sums on the batch with
+        every budget scaled by ``scale``.  The tally modes are then timed on
+        the best shape at ``mode_scale``: contention on one problem's sums
+        grows with the photons of that problem in flight at once, so the
+        comparison needs budgets closer to the real ones (measured on C5:
+        equal at 1/64, 1.3 % apart at 1/8, global atomics 25 % slower at
+        full size).  Arguments
+        that are set (non-zero, not None) are kept as given."""
         sig = (torch.cuda.get_device_name(self.device), self.P,
-               int(self.host_slabs["photons"].sum()), round(float(self.host_slabs["ma"].mean()), 6))
+               int(self.host_slabs["photons"].sum()), round(float(self.host_slabs["ma"].mean()), 6),
+               block_threads, chunk, tally_mode)
         if sig in _TUNE_CACHE:
-            return _TUNE_CACHE[sig]
+            self.tune_table = _TUNE_CACHE[sig]
+            return self.tune_table["best"]
         if candidates is None:
-            candidates = [(t, c) for t in (64, 128, 256) for c in (64, 512, 4096)]
+            candidates = [(t, c) for t in ((block_threads,) if block_threads else (64, 128, 256))
+                          for c in ((chunk,) if chunk else (64, 512, 4096))]
+        modes = (tally_mode,) if tally_mode is not None else (A.PMO_BT_THREAD, A.PMO_BT_GLOBAL)
         dev = self.device
-        small = self.host_slabs.copy()
-        small["photons"] = np.maximum(1, (small["photons"] * scale).astype(np.int64))
-        slabs = torch.from_numpy(small.view(np.uint8).copy()).to(dev)
         sums = torch.zeros_like(self.sums)
         bins = torch.zeros_like(self.bins)
         rem = torch.zeros_like(self.remaining)
         tdone = torch.zeros_like(self.t_done)
         lib = load()
-        best, best_t = None, float("inf")
-        for threads, chunk in candidates:
-            items = build_items(small["photons"], chunk)
+
+        def scaled(f):
+            small = self.host_slabs.copy()
+            small["photons"] = np.maximum(1, (small["photons"] * f).astype(np.int64))
+            return small["photons"], torch.from_numpy(small.view(np.uint8).copy()).to(dev)
+
+        def timed(photons, slabs, threads, chunk, mode):
+            items = build_items(photons, chunk)
             d_items = torch.from_numpy(items.view(np.uint8).copy()).to(dev)
             b = self._struct(slabs=slabs, items=d_items, n_items=len(items), sums=sums,
-                             bins=bins, remaining=rem, t_done=tdone)
+                             bins=bins, remaining=rem, t_done=tdone, tally_mode=mode)
             times = []
             for rep in range(3):
                 e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -216,11 +240,26 @@ class SlabBatch:
                 torch.cuda.synchronize()
                 if rep:
                     times.append(e0.elapsed_time(e1))
-            t = min(times)
-            if t < best_t:
-                best, best_t = (threads, chunk), t
-        _TUNE_CACHE[sig] = best
-        self.tune_table = {"best": best, "best_ms": best_t}
+            return min(times)
+
+        small = scaled(scale)
+        shapes = {(t, c): timed(*small, t, c, modes[0]) for t, c in candidates}
+        shape = min(shapes, key=shapes.get)
+        if len(modes) > 1:
+            mid = scaled(mode_scale)
+            by_mode = {m: timed(*mid, *shape, m) for m in modes}
+        else:
+            by_mode = {modes[0]: shapes[shape]}
+        # contention only grows with the budgets, so the down-scaled timing
+        # flatters global atomics: they must win clearly to be kept
+        mode = modes[0]
+        if len(modes) > 1 and by_mode[A.PMO_BT_GLOBAL] < 0.97 * by_mode[A.PMO_BT_THREAD]:
+            mode = A.PMO_BT_GLOBAL
+        best = (*shape, mode)
+        self.tune_table = {"best": best, "shape_ms": {str(k): v for k, v in shapes.items()},
+                           "mode_ms": {("thread" if m == A.PMO_BT_THREAD else "global"): v
+                                       for m, v in by_mode.items()}}
+        _TUNE_CACHE[sig] = self.tune_table
         return best
 
 
@@ -296,7 +335,8 @@ def batched_vs_plain(count: int = 4096, plain_sample: int = 48, seed: int = 0, n
     singles = [SlabBatch([b["ma"][i]], [b["ms"][i]], [b["g"][i]], [b["n"][i]],
                          [b["thickness"][i]], [int(b["n_photons"][i])], nr=nr, dr=dr,
                          seed=seed + 1, device=device, autotune=False,
-                         block_threads=sb.block_threads, chunk=sb.chunk) for i in pick]
+                         block_threads=sb.block_threads, chunk=sb.chunk,
+                         tally_mode=sb.tally_mode) for i in pick]
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for one in singles:
@@ -318,7 +358,9 @@ def batched_vs_plain(count: int = 4096, plain_sample: int = 48, seed: int = 0, n
         "ratio_vs_single_launches": tb["evals_per_s"] / single_rate,
         "p50_completion_ms": float(np.percentile(comp, 50)),
         "p99_completion_ms": float(np.percentile(comp, 99)),
-        "launch_shape": {"block_threads": sb.block_threads, "photons_per_item": sb.chunk},
+        "launch_shape": {"block_threads": sb.block_threads, "photons_per_item": sb.chunk,
+                         "tally_mode": "thread" if sb.tally_mode == A.PMO_BT_THREAD
+                         else "global"},
         "autotune_seconds": tune_s,
         "max_energy_residual": float(np.max(np.abs(res["balance"]))),
     }
@@ -337,18 +379,22 @@ def main(argv=None) -> int:
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--block-threads", type=int, default=0)
     ap.add_argument("--chunk", type=int, default=0, help="photons per work item")
+    ap.add_argument("--tally-mode", choices=["auto", "thread", "global"], default="auto",
+                    help="per-problem sums privatised per thread, or straight to global memory")
     args = ap.parse_args(argv)
     b = V.c5_slab_batch(seed=0, count=args.count)
     photons = np.maximum(1, (b["n_photons"] * args.photon_scale).astype(np.int64))
+    mode = {"auto": None, "thread": A.PMO_BT_THREAD, "global": A.PMO_BT_GLOBAL}[args.tally_mode]
     sb = SlabBatch(b["ma"], b["ms"], b["g"], b["n"], b["thickness"], photons, nr=32, dr=0.1,
-                   seed=1, autotune=not (args.block_threads and args.chunk),
-                   block_threads=args.block_threads, chunk=args.chunk)
+                   seed=1, block_threads=args.block_threads, chunk=args.chunk, tally_mode=mode)
     tb = time_batch(sb, reps=args.reps)
     res = sb.fetch()
     print(json.dumps({"problems": sb.P, "photons": float(photons.sum()),
                       "seconds": tb["seconds"], "evals_per_s": tb["evals_per_s"],
                       "photons_per_s": float(photons.sum()) / tb["seconds"],
                       "block_threads": sb.block_threads, "photons_per_item": sb.chunk,
+                      "tally_mode": "thread" if sb.tally_mode == A.PMO_BT_THREAD else "global",
+                      "autotune": getattr(sb, "tune_table", None),
                       "p50_completion_ms": float(np.percentile(res["completion_ms"], 50)),
                       "p99_completion_ms": float(np.percentile(res["completion_ms"], 99)),
                       "max_energy_residual": float(np.max(np.abs(res["balance"])))}))

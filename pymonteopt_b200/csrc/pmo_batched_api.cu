@@ -65,6 +65,7 @@ int pmo_run_batched(const pmo_batch *b, const pmo_launch *launch, void *workspac
         return PMO_ERR_ARG;
     if (b->nr < 0 || (b->nr > 0 && !b->bins)) return PMO_ERR_ARG;
     if (b->precision != PMO_FP32 && b->precision != PMO_FP64) return PMO_ERR_ARG;
+    if (b->tally_mode != PMO_BT_THREAD && b->tally_mode != PMO_BT_GLOBAL) return PMO_ERR_ARG;
     if (!workspace || workspace_bytes < kWorkspaceBytes) return PMO_ERR_WORKSPACE;
     const int threads = launch && launch->block_threads > 0 ? launch->block_threads : 128;
     if (threads % 32 != 0 || threads > 512) return PMO_ERR_ARG;
@@ -90,6 +91,7 @@ int pmo_run_batched(const pmo_batch *b, const pmo_launch *launch, void *workspac
     bp.remaining = b->remaining;
     bp.t_done = b->t_done;
     bp.max_events = b->max_events;
+    bp.tally_mode = b->tally_mode;
     bp.work = work;
     const cudaError_t e = b->precision == PMO_FP64 ? pmo::launch_batched_f64(bp, threads, bps, s)
                                                    : pmo::launch_batched_f32(bp, threads, bps, s);

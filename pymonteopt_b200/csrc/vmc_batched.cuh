@@ -12,8 +12,12 @@
 // photon starts the next at once, whatever problem it belongs to, so the
 // launch stays full across thousands of problems with uneven budgets.  Each
 // lane keeps the problem parameters of its own photon.  Per-problem sums are
-// privatised per thread in shared memory and flushed when the thread moves
-// on to another problem.
+// either privatised per thread in shared memory and flushed when the thread
+// moves on to another problem (PMO_BT_THREAD), or added to global memory as
+// they occur (PMO_BT_GLOBAL); the batch autotuner times both.  A photon's
+// absorbed weight is summed per segment (start or last roulette gain to the
+// next roulette or the end) as the weight it lost, so no sum is touched per
+// interaction.
 //
 // Forward and gradient in one pass: with one layer the perturbation Monte
 // Carlo derivative of an exit weight needs only the photon's total path
@@ -36,6 +40,7 @@ struct BParams {
     uint32_t *remaining;
     unsigned long long *t_done;
     uint32_t max_events;
+    int32_t tally_mode;           // PMO_BT_THREAD or PMO_BT_GLOBAL
     unsigned long long *work;     // [0] next item, [1] launch start time
 };
 
@@ -54,43 +59,53 @@ enum : int {
 template <typename R>
 __global__ void __launch_bounds__(512) vmc_batched_kernel(const BParams bp) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    const bool priv = bp.tally_mode == PMO_BT_THREAD;
     double *acc = reinterpret_cast<double *>(smem_raw) + threadIdx.x * kSlots;
-    for (int i = 0; i < kSlots; ++i) acc[i] = 0.0;
+    if (priv)
+        for (int i = 0; i < kSlots; ++i) acc[i] = 0.0;
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicMin(bp.work + 1, global_ns());
 
     const unsigned FULL = 0xffffffffu;
     const unsigned lane = threadIdx.x & 31u;
     const uint32_t cap = bp.max_events ? bp.max_events : (1u << 26);
+    const int map[12] = {PMO_BS_RD, PMO_BS_RD_L, PMO_BS_RD_N, PMO_BS_TT, PMO_BS_TT_L,
+                         PMO_BS_TT_N, PMO_BS_ABS, PMO_BS_WINIT, PMO_BS_RGAIN, PMO_BS_RLOSS,
+                         PMO_BS_ERRW, PMO_BS_INTER};
 
+    // photons of problem pp ended: count them down, stamp the completion time
+    auto complete = [&](int pp, uint32_t done) {
+        if (bp.remaining && done) {
+            const uint32_t before = atomicSub(bp.remaining + pp, done);
+            if (before == done && bp.t_done) bp.t_done[pp] = global_ns();
+        }
+    };
     int acc_p = -1;  // problem held in acc[]
     auto flush = [&]() {
         if (acc_p < 0) return;
         double *dst = bp.sums + (size_t)acc_p * PMO_BS_N;
-        const int map[12] = {PMO_BS_RD, PMO_BS_RD_L, PMO_BS_RD_N, PMO_BS_TT, PMO_BS_TT_L,
-                             PMO_BS_TT_N, PMO_BS_ABS, PMO_BS_WINIT, PMO_BS_RGAIN, PMO_BS_RLOSS,
-                             PMO_BS_ERRW, PMO_BS_INTER};
 #pragma unroll
         for (int i = 0; i < 12; ++i)
             if (acc[i] != 0.0) atomicAdd(dst + map[i], acc[i]);
-        const uint32_t done = (uint32_t)acc[kSlotDone];
-        if (bp.remaining && done) {
-            const uint32_t before = atomicSub(bp.remaining + acc_p, done);
-            if (before == done && bp.t_done) bp.t_done[acc_p] = global_ns();
-        }
+        complete(acc_p, (uint32_t)acc[kSlotDone]);
         for (int i = 0; i < kSlots; ++i) acc[i] = 0.0;
         acc_p = -1;
     };
 
-    // photon state
+    // photon state; wseg: weight at the start of the absorption segment
     int p = -1;
     uint32_t j = 0, k = 0, f = 0, ncr = 0;
-    R x = 0, y = 0, z = 0, vx = 0, vy = 0, vz = 1, w = 0, L = 0, n_int = 0;
+    R x = 0, y = 0, z = 0, vx = 0, vy = 0, vz = 1, w = 0, wseg = 0, L = 0;
+    // add v to sum `slot` of the photon's problem
+    auto add = [&](int slot, double v) {
+        if (priv) acc[slot] += v;
+        else if (v != 0.0) atomicAdd(bp.sums + (size_t)p * PMO_BS_N + map[slot], v);
+    };
     // problem constants of the photon in flight
     R mt = 0, imt = 0, ma_mt = 0, ims = 0, nin = 1, nout = 1, th = 1, dr = 1;
     LabelProps<R> hg;
 
     auto start = [&](int pp, uint32_t jj) -> bool {
-        if (pp != acc_p) {
+        if (priv && pp != acc_p) {
             flush();
             acc_p = pp;
         }
@@ -119,13 +134,16 @@ __global__ void __launch_bounds__(512) vmc_batched_kernel(const BParams bp) {
         x = y = z = R(0);
         vx = vy = R(0);
         vz = R(1);
-        L = n_int = R(0);
-        acc[kSlotWinit] += (double)w;
+        wseg = w;
+        L = R(0);
+        add(kSlotWinit, (double)w);
         return true;
     };
     auto finish = [&]() {
-        acc[kSlotDone] += 1.0;
-        acc[kSlotInter] += (double)k;
+        add(kSlotAbs, (double)wseg - (double)w);
+        add(kSlotInter, (double)k);
+        if (priv) acc[kSlotDone] += 1.0;
+        else complete(p, 1u);
     };
 
     // one interaction cycle; returns true while the photon is in flight
@@ -153,7 +171,7 @@ __global__ void __launch_bounds__(512) vmc_batched_kernel(const BParams bp) {
             st = xsub(st, dbmt);
             ++ncr;
             if (ncr + k - 1 > cap) {
-                acc[kSlotErr] += (double)w;
+                add(kSlotErr, (double)w);
                 finish();
                 return false;
             }
@@ -203,12 +221,13 @@ __global__ void __launch_bounds__(512) vmc_batched_kernel(const BParams bp) {
                 vy = xmul(vy, inv);
                 vz = xmul(vz, inv);
             }
+            // interactions so far: every earlier cycle ended in one
             const double wd = (double)w;
-            const double wl = wd * (double)L, wn = wd * (double)n_int;
+            const double wl = wd * (double)L, wn = wd * (double)(k - 1u);
             if (vz < R(0)) {
-                acc[kSlotRd] += wd;
-                acc[kSlotRdL] += wl;
-                acc[kSlotRdN] += wn;
+                add(kSlotRd, wd);
+                add(kSlotRdL, wl);
+                add(kSlotRdN, wn);
                 // R(r) of the exit point around the entry point
                 const R r = psqrt(xfma(y, y, xmul(x, x)));
                 if (r > R(0) && bp.nr > 0) {
@@ -221,30 +240,26 @@ __global__ void __launch_bounds__(512) vmc_batched_kernel(const BParams bp) {
                     }
                 }
             } else {
-                acc[kSlotTt] += wd;
-                acc[kSlotTtL] += wl;
-                acc[kSlotTtN] += wn;
+                add(kSlotTt, wd);
+                add(kSlotTtL, wl);
+                add(kSlotTtN, wn);
             }
             finish();
             return false;
         }
         // absorption (:179)
-        {
-            const R wn = xfma(-w, ma_mt, w);
-            acc[kSlotAbs] += (double)w - (double)wn;
-            w = wn;
-        }
-        n_int = xadd(n_int, R(1));
+        w = xfma(-w, ma_mt, w);
         // roulette (:182-195)
         if (w <= R(0.0001)) {
             if (R(0.1) < u01<R>(rn.y)) {
-                acc[kSlotLoss] += (double)w;
+                add(kSlotLoss, (double)w);
                 finish();
                 return false;
             }
+            add(kSlotAbs, (double)wseg - (double)w);
             const R wn = xmul(w, R(10));
-            acc[kSlotGain] += (double)wn - (double)w;
-            w = wn;
+            add(kSlotGain, (double)wn - (double)w);
+            w = wseg = wn;
         }
         // spin (:197-219)
         {
@@ -274,7 +289,7 @@ __global__ void __launch_bounds__(512) vmc_batched_kernel(const BParams bp) {
             vz = xmul(vz, inv);
         }
         if (ncr + k > cap) {
-            acc[kSlotErr] += (double)w;
+            add(kSlotErr, (double)w);
             finish();
             return false;
         }

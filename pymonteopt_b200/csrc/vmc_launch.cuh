@@ -95,7 +95,8 @@ cudaError_t launch_grad_r(const KParams &kp, int props, int threads, int bps, cu
 template <typename R>
 cudaError_t launch_batched_r(const BParams &bp, int threads, int blocks_per_sm, cudaStream_t s) {
     auto kern = vmc_batched_kernel<R>;
-    const size_t smem = (size_t)threads * kSlots * sizeof(double);
+    const size_t smem =
+        bp.tally_mode == PMO_BT_THREAD ? (size_t)threads * kSlots * sizeof(double) : 0;
     cudaError_t e;
     if (smem > 48 * 1024) {
         e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -130,3 +130,26 @@ def test_batch_ledger_completion_and_graph(cuda):
     np.testing.assert_allclose(graphed["Rr"], direct["Rr"], rtol=1e-4, atol=1e-9)
     again = sb.run(use_graph=True)
     np.testing.assert_allclose(again["Tt"], graphed["Tt"], rtol=1e-6)
+
+
+def test_tally_modes_agree_and_autotuner_picks_one(cuda):
+    """Per-thread privatised sums and direct global atomics see the same
+    photons; the autotuner times both and keeps one."""
+    b = V.c5_slab_batch(seed=5, count=48)
+    photons = np.maximum(500, b["n_photons"] // 200)
+    common = dict(nr=16, dr=0.2, seed=9, autotune=False, block_threads=128, chunk=64)
+    runs = {}
+    for mode in (A.PMO_BT_THREAD, A.PMO_BT_GLOBAL):
+        sb = B.SlabBatch(b["ma"], b["ms"], b["g"], b["n"], b["thickness"], photons,
+                         tally_mode=mode, **common)
+        runs[mode] = sb.run(use_graph=False)
+        assert np.all(sb.remaining.cpu().numpy() == 0)
+        assert np.all(runs[mode]["completion_ms"] > 0)
+    t, g = runs[A.PMO_BT_THREAD], runs[A.PMO_BT_GLOBAL]
+    np.testing.assert_allclose(g["sums"], t["sums"], rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(g["Rr"], t["Rr"], rtol=1e-5, atol=1e-9)
+    assert np.all(np.abs(g["balance"]) < 1e-9)
+    tuned = B.SlabBatch(b["ma"], b["ms"], b["g"], b["n"], b["thickness"], photons, nr=16,
+                        dr=0.2, seed=9, block_threads=128, chunk=64)
+    assert tuned.tally_mode in (A.PMO_BT_THREAD, A.PMO_BT_GLOBAL)
+    assert set(tuned.tune_table["mode_ms"]) == {"thread", "global"}
