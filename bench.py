@@ -57,6 +57,8 @@ def parse_args():
     ap.add_argument("--ref-gpu-photons", type=float, default=1e7)
     ap.add_argument("--no-gradient", action="store_true",
                     help="skip timing the differentiable form (64^3 per-voxel optics)")
+    ap.add_argument("--no-precision", action="store_true",
+                    help="skip the FP32-vs-FP64 error of the results (1e6 photons, C1 and C2)")
     ap.add_argument("--block-threads", type=int, default=0)
     ap.add_argument("--blocks-per-sm", type=int, default=0)
     return ap.parse_args()
@@ -335,6 +337,49 @@ def gradient_leg(torch, dev, photons: int = 10_000_000, evals: int = 3) -> dict:
             "grad_finite": bool(torch.isfinite(ma_.grad).all() and torch.isfinite(ms_.grad).all())}
 
 
+def precision_leg(torch, dev, photons: int = 1_000_000) -> dict:
+    """Error of the FP32 product against the FP64 build of the same kernel on
+    identical Philox streams (the per-photon oracle): Rd, Tt, A, R(r) and the
+    absorbed grid, on C1 (with the fluence tally) and on this workload (C2)."""
+    from pymonteopt_b200 import _abi as A
+    from pymonteopt_b200 import engine as E
+    from pymonteopt_b200 import volumes as V
+    out = {"photons": photons}
+    for name, prob, flu in (("c1_slab", V.c1_slab(), A.PMO_FLU_GLOBAL),
+                            ("c2_skin", V.c2_skin(), A.PMO_FLU_NONE)):
+        dp = E.DeviceProblem(prob, dev)
+        runs = {}
+        for prec in (A.PMO_FP32, A.PMO_FP64):
+            spec = E.TallySpec(nr=100, dr=0.1, fluence=flu, photon_stats=True)
+            t = E.run_plain(dp, photons, 4242, spec=spec, precision=prec)
+            torch.cuda.synchronize()
+            t.check()
+            runs[prec] = t
+        t32, t64 = runs[A.PMO_FP32], runs[A.PMO_FP64]
+        s32, s64 = t32.summary(), t64.summary()
+        r = {}
+        for key in ("Rd", "Tt", "A"):
+            r[key] = {"fp32": float(s32[key]), "fp64": float(s64[key]),
+                      "abs_err": float(abs(s32[key] - s64[key]))}
+        # Rd's standard error from the run itself, for scale
+        r["Rd"]["binomial_se"] = float(np.sqrt(max(s64["Rd"] * (1 - s64["Rd"]), 0.0) / photons))
+        rr32 = t32.rr.double()[A.PMO_RR_TOP]
+        rr64 = t64.rr.double()[A.PMO_RR_TOP]
+        r["Rr_top"] = {"rel_l1_err": float((rr32 - rr64).abs().sum() / rr64.abs().sum()),
+                       "max_abs_err_of_max": float((rr32 - rr64).abs().max() / rr64.abs().max())}
+        same = (t32.ph[0] == t64.ph[0]) & (t32.ph[2] == t64.ph[2])
+        r["same_event_counts_share"] = float(same.double().mean())
+        if flu != A.PMO_FLU_NONE:
+            g32, g64 = E.absorbed_weight(t32), E.absorbed_weight(t64)
+            hot = g64 >= 0.01 * g64.max()
+            r["absorbed"] = {
+                "rel_l2_err": float((g32 - g64).norm() / g64.norm()),
+                "max_rel_err_hot_voxels": float(((g32 - g64).abs()[hot] / g64[hot]).max()),
+                "hot_voxels": int(hot.sum())}
+        out[name] = r
+    return out
+
+
 # ---------------------------------------------------------------------------
 def fp32_probe(torch, lib) -> float:
     """Measured FP32 issue rate (FFMA thread-instructions per second)."""
@@ -536,6 +581,10 @@ def main() -> int:
     if rank == 0 and world == 1 and not args.no_gradient:
         gradient = gradient_leg(torch, dev)
 
+    precision = None
+    if rank == 0 and world == 1 and not args.no_precision:
+        precision = precision_leg(torch, dev)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = cpu_oracle_rate(12.0)
@@ -562,6 +611,7 @@ def main() -> int:
         "batched": batched,
         "reference_gpu": reference_gpu,
         "gradient": gradient,
+        "fp32_vs_fp64": precision,
         "clocks": clk,
         "wall_s_timed_region": wall,
         "results": results,
