@@ -5,7 +5,10 @@
 // This restates the reference's vectorised NumPy ray tracing
 // (pymopt/optics/_classes.py:50-380 for the elements, :454-526 for the
 // scan, :528-566 for the side geometry) per photon:
-// - one thread per exit photon, looping over the scan;
+// - one thread per exit photon, looping over the scan; photons that miss
+//   lens 1 at every Z are dropped by an exact-safe test first, and each
+//   block gathers the rest in a shared queue, so that a scan round gives
+//   every thread a photon that may pass;
 // - the intensity of each Z summed in shared memory, then one FP64 atomic
 //   per block and Z.
 //
@@ -161,113 +164,232 @@ __device__ __forceinline__ bool ld_mount(Ray &r, double front, double back, doub
 }
 
 constexpr int kMaxZ = 4096;
+constexpr int kObdThreads = 256;
 
-__global__ void __launch_bounds__(256, 4) obd_kernel(pmo_obd_params prm, const float *__restrict__ p,
-                                                  const float *__restrict__ v,
-                                                  const float *__restrict__ w, int64_t n,
-                                                  double *__restrict__ intensity) {
-    extern __shared__ double s_int[];
-    for (int i = threadIdx.x; i < prm.n_z; i += blockDim.x) s_int[i] = 0.0;
-    __syncthreads();
-    const pmo::PhiloxKeys rk = pmo::philox_round_keys((uint32_t)prm.seed,
-                                                      (uint32_t)(prm.seed >> 32));
-    const double d_out = prm.slit_d / 2 + prm.slit_width / 2;
-    const double d_in = prm.slit_d / 2 - prm.slit_width / 2;
-    // mount edges: angle 68/180 rad, thickness 5, width 6 (:338-350)
-    const double ang = 68.0 / 180.0;
-    const double a1 = 1.0 / tan(ang) - 1.0 / (sin(ang) * cos(ang));
-    const double b1 = 6.0 / cos(ang);
-    const double a2 = (cos(ang) + 1.0) / sin(ang);
-    const double b2 = -6.0, b3 = -6.0;
-    // total-internal-reflection thresholds asin(nt / ni) of the glass-to-air
-    // surfaces (:176)
-    const double tir1 = asin(1.0 / prm.n1), tir2 = asin(1.0 / prm.n2);
+// Constants of one scan, shared by every photon.
+struct ScanConsts {
+    double d_in, d_out;                 // annular slit radii
+    double a1, b1, a2, b2, b3;          // laser-diode mount edges
+    double tir1, tir2;                  // total-internal-reflection thresholds
+    double zlo, zhi;                    // smallest and largest Z of the scan
+    pmo::PhiloxKeys rk;
+};
 
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        const float x0 = p[i], y0 = p[n + i];
-        // the first normalisation of v is in float32, like its input
-        const float vx0 = v[i], vy0 = v[n + i], vz0 = v[2 * n + i];
-        const float vs = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(vx0, vx0), __fmul_rn(vy0, vy0)),
-                                              __fmul_rn(vz0, vz0)));
-        const double ux = (double)__fdiv_rn(vx0, vs), uy = (double)__fdiv_rn(vy0, vs),
-                     uz = (double)__fdiv_rn(vz0, vs);
-        const double wi = (double)w[i];
-        // Lens 1's flat face has the fixed normal (0, 0, -1): the incidence
-        // angle, the reflectance and the refracted direction do not depend on
-        // Z, only the hit point and the draw do.  Computed once per photon,
-        // with the same operations as inside the scan.
-        Ray r1;
-        r1.px = r1.py = r1.pz = 0.0;
-        r1.vx = ux;
-        r1.vy = uy;
-        r1.vz = uz;
-        Cosines c1;
-        refract(r1, 0.0, 0.0, -1.0, prm.n1, false, 0.0, c1);
-        const double R1 = reflectance(c1);
-        normalize(r1);
-        for (int zi = 0; zi < prm.n_z; ++zi) {
-            const double Z = prm.z[zi];
-            // element positions of this Z (:454-470)
-            const double zl1 = -prm.bfl1 + Z;
-            const double zl2 = zl1 - prm.ct1 - prm.slit_thickness * 2 - prm.ct2 - prm.distance_2slits;
-            const double zs1 = zl1 - prm.ct1;
-            const double zs2 = zl2 + prm.ct2 + prm.slit_thickness;
-            const double zpd = zl2 - prm.bfl2 - prm.pd_correction;
-            Ray r;
-            r.px = prm.side ? (double)(float)((double)x0 - (Z + prm.side_dz) * prm.side_tan)
-                            : (double)x0;
-            r.py = (double)y0;
-            r.pz = 0.0;
-            r.vx = ux;
-            r.vy = uy;
-            r.vz = uz;
-            // lens 1: flat face (the float32-normalised v goes in as it is)
-            // then curved face (:295-302)
-            hit_plane(r, zl1);
-            if (!(radius(r) <= prm.outer_d1 / 2)) continue;
-            r.vx = r1.vx;
-            r.vy = r1.vy;
-            r.vz = r1.vz;
-            Cosines c2, c3, c4;
-            if (!convex(r, zl1 - (prm.ct1 - prm.r1), prm.r1, false, prm.outer_d1 / 2, prm.n1,
-                        tir1, c2))
-                continue;
-            if (!slit(r, zs1, zs1 - prm.slit_thickness, d_in, d_out)) continue;
-            if (prm.ld_fix_part) {
-                const double zf = zs1 - prm.slit_thickness - 10;
-                if (!ld_mount(r, zf, zf - 5, a1, b1, a2, b2, b3)) continue;
-            }
-            if (!slit(r, zs2, zs2 - prm.slit_thickness, d_in, d_out)) continue;
-            // lens 2: curved face then flat face (:305-313)
-            if (!convex(r, zl2 + (prm.ct2 - prm.r2), prm.r2, true, prm.outer_d2 / 2, prm.n2,
-                        0.0, c3))
-                continue;
-            if (!plano_out(r, zl2, prm.outer_d2 / 2, prm.n2, tir2, c4)) continue;
-            // photodiode (:325-334)
-            hit_plane(r, zpd);
-            if (!(radius(r) < prm.d_pd / 2)) continue;
-            // the four Fresnel decisions, which do not change the ray: drawn
-            // and taken only for photons that reach the photodiode
-            double u[4];
-            if (prm.fixed_u >= 0.0) {
-                u[0] = u[1] = u[2] = u[3] = prm.fixed_u;
-            } else {
-                const uint4 q = pmo::philox4x32_10(
-                    make_uint4((uint32_t)zi, 5u, (uint32_t)i, (uint32_t)((uint64_t)i >> 32)), rk);
-                u[0] = (double)q.x * 0x1p-32;
-                u[1] = (double)q.y * 0x1p-32;
-                u[2] = (double)q.z * 0x1p-32;
-                u[3] = (double)q.w * 0x1p-32;
-            }
-            if (!passes(u[0], R1) || !passes(u[1], reflectance(c2)) ||
-                !passes(u[2], reflectance(c3)) || !passes(u[3], reflectance(c4)))
-                continue;
-            atomicAdd(s_int + zi, wi);
+// The exit photon's direction, normalised in float32 like its input.
+__device__ __forceinline__ void exit_direction(const float *v, int64_t n, int64_t i, double &ux,
+                                               double &uy, double &uz) {
+    const float vx0 = v[i], vy0 = v[n + i], vz0 = v[2 * n + i];
+    const float vs = __fsqrt_rn(__fadd_rn(__fadd_rn(__fmul_rn(vx0, vx0), __fmul_rn(vy0, vy0)),
+                                          __fmul_rn(vz0, vz0)));
+    ux = (double)__fdiv_rn(vx0, vs);
+    uy = (double)__fdiv_rn(vy0, vs);
+    uz = (double)__fdiv_rn(vz0, vs);
+}
+
+// Whether photon i can pass lens 1's aperture for some Z of the scan.  Its
+// hit point on lens 1's plane is affine in Z, A + B Z (the plane sits at
+// Z - bfl1; the side geometry's x shift is affine in Z too), so the distance
+// from the axis is convex in Z and smallest at the clamped vertex Z*.  The
+// test uses an aperture 1 um wider than the lens, far more than the rounding
+// of the exact per-Z test (and of the side geometry's float32 x), so it only
+// drops photons that the exact test rejects at every Z.  A direction with
+// v_z = 0 or a zero vector gives NaN, which no Z passes either.
+__device__ __forceinline__ bool reaches_lens1(const pmo_obd_params &prm, const ScanConsts &k,
+                                              const float *p, const float *v, const float *w,
+                                              int64_t n, int64_t i) {
+    if (!(w[i] != 0.0f)) return false;   // adds nothing to any Z
+    double ux, uy, uz;
+    exit_direction(v, n, i, ux, uy, uz);
+    const double iz = 1.0 / uz;
+    const double st = prm.side ? prm.side_tan : 0.0;
+    const double bx = ux * iz - st, by = uy * iz;
+    const double ax = (double)p[i] - (prm.side ? prm.side_dz * st : 0.0) - prm.bfl1 * ux * iz;
+    const double ay = (double)p[n + i] - prm.bfl1 * uy * iz;
+    const double bb = bx * bx + by * by;
+    double zs = bb > 0.0 ? -(ax * bx + ay * by) / bb : k.zlo;
+    zs = fmin(fmax(zs, k.zlo), k.zhi);
+    const double qx = ax + bx * zs, qy = ay + by * zs;
+    const double rm = prm.outer_d1 / 2 + 1e-3;
+    return qx * qx + qy * qy <= rm * rm;
+}
+
+// Photon i through the bench for every Z of the scan; each Z that reaches the
+// photodiode and passes the four Fresnel decisions adds w_i to s_int[Z].
+__device__ void scan_photon(const pmo_obd_params &prm, const ScanConsts &k, const float *p,
+                            const float *v, const float *w, int64_t n, int64_t i,
+                            double *s_int) {
+    const float x0 = p[i], y0 = p[n + i];
+    double ux, uy, uz;
+    exit_direction(v, n, i, ux, uy, uz);
+    const double wi = (double)w[i];
+    // Lens 1's flat face has the fixed normal (0, 0, -1): the incidence
+    // angle, the reflectance and the refracted direction do not depend on
+    // Z, only the hit point and the draw do.  Computed once per photon,
+    // with the same operations as inside the scan.
+    Ray r1;
+    r1.px = r1.py = r1.pz = 0.0;
+    r1.vx = ux;
+    r1.vy = uy;
+    r1.vz = uz;
+    Cosines c1;
+    refract(r1, 0.0, 0.0, -1.0, prm.n1, false, 0.0, c1);
+    const double R1 = reflectance(c1);
+    normalize(r1);
+    for (int zi = 0; zi < prm.n_z; ++zi) {
+        const double Z = prm.z[zi];
+        // element positions of this Z (:454-470)
+        const double zl1 = -prm.bfl1 + Z;
+        const double zl2 = zl1 - prm.ct1 - prm.slit_thickness * 2 - prm.ct2 - prm.distance_2slits;
+        const double zs1 = zl1 - prm.ct1;
+        const double zs2 = zl2 + prm.ct2 + prm.slit_thickness;
+        const double zpd = zl2 - prm.bfl2 - prm.pd_correction;
+        Ray r;
+        r.px = prm.side ? (double)(float)((double)x0 - (Z + prm.side_dz) * prm.side_tan)
+                        : (double)x0;
+        r.py = (double)y0;
+        r.pz = 0.0;
+        r.vx = ux;
+        r.vy = uy;
+        r.vz = uz;
+        // lens 1: flat face (the float32-normalised v goes in as it is)
+        // then curved face (:295-302)
+        hit_plane(r, zl1);
+        if (!(radius(r) <= prm.outer_d1 / 2)) continue;
+        r.vx = r1.vx;
+        r.vy = r1.vy;
+        r.vz = r1.vz;
+        Cosines c2, c3, c4;
+        if (!convex(r, zl1 - (prm.ct1 - prm.r1), prm.r1, false, prm.outer_d1 / 2, prm.n1,
+                    k.tir1, c2))
+            continue;
+        if (!slit(r, zs1, zs1 - prm.slit_thickness, k.d_in, k.d_out)) continue;
+        if (prm.ld_fix_part) {
+            const double zf = zs1 - prm.slit_thickness - 10;
+            if (!ld_mount(r, zf, zf - 5, k.a1, k.b1, k.a2, k.b2, k.b3)) continue;
         }
+        if (!slit(r, zs2, zs2 - prm.slit_thickness, k.d_in, k.d_out)) continue;
+        // lens 2: curved face then flat face (:305-313)
+        if (!convex(r, zl2 + (prm.ct2 - prm.r2), prm.r2, true, prm.outer_d2 / 2, prm.n2,
+                    0.0, c3))
+            continue;
+        if (!plano_out(r, zl2, prm.outer_d2 / 2, prm.n2, k.tir2, c4)) continue;
+        // photodiode (:325-334)
+        hit_plane(r, zpd);
+        if (!(radius(r) < prm.d_pd / 2)) continue;
+        // the four Fresnel decisions, which do not change the ray: drawn
+        // and taken only for photons that reach the photodiode
+        double u[4];
+        if (prm.fixed_u >= 0.0) {
+            u[0] = u[1] = u[2] = u[3] = prm.fixed_u;
+        } else {
+            const uint4 q = pmo::philox4x32_10(
+                make_uint4((uint32_t)zi, 5u, (uint32_t)i, (uint32_t)((uint64_t)i >> 32)), k.rk);
+            u[0] = (double)q.x * 0x1p-32;
+            u[1] = (double)q.y * 0x1p-32;
+            u[2] = (double)q.z * 0x1p-32;
+            u[3] = (double)q.w * 0x1p-32;
+        }
+        if (!passes(u[0], R1) || !passes(u[1], reflectance(c2)) ||
+            !passes(u[2], reflectance(c3)) || !passes(u[3], reflectance(c4)))
+            continue;
+        atomicAdd(s_int + zi, wi);
+    }
+}
+
+// Each block walks its tiles of kObdThreads photons, keeps the photons that
+// can reach lens 1 in a shared queue, and scans them kObdThreads at a time,
+// so that every thread of a scan round holds a photon that may pass.  (About
+// 60 % of Lambertian exits miss lens 1 at every Z of the default scan; with
+// one photon per thread their lanes would idle through all of it.)  Every
+// barrier sits in control flow that is uniform over the block: the queue
+// count is read after a barrier and the tile index is the same in all
+// threads.
+__global__ void __launch_bounds__(kObdThreads, 4) obd_kernel(pmo_obd_params prm,
+                                                             const float *__restrict__ p,
+                                                             const float *__restrict__ v,
+                                                             const float *__restrict__ w,
+                                                             int64_t n,
+                                                             double *__restrict__ intensity) {
+    extern __shared__ double s_int[];
+    __shared__ int64_t s_idx[2 * kObdThreads];
+    __shared__ int s_count;
+    __shared__ double s_zlo[kObdThreads / 32], s_zhi[kObdThreads / 32];
+    __shared__ ScanConsts s_k;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < prm.n_z; i += blockDim.x) s_int[i] = 0.0;
+    // the scan's Z range
+    double lo = prm.z[0], hi = prm.z[0];
+    for (int i = tid; i < prm.n_z; i += blockDim.x) {
+        lo = fmin(lo, prm.z[i]);
+        hi = fmax(hi, prm.z[i]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if ((tid & 31) == 0) {
+        s_zlo[tid >> 5] = lo;
+        s_zhi[tid >> 5] = hi;
+    }
+    if (tid == 0) {
+        s_count = 0;
+        // scan constants, read from shared memory by every thread (in
+        // registers they would spill)
+        ScanConsts &k = s_k;
+        k.rk = pmo::philox_round_keys((uint32_t)prm.seed, (uint32_t)(prm.seed >> 32));
+        k.d_out = prm.slit_d / 2 + prm.slit_width / 2;
+        k.d_in = prm.slit_d / 2 - prm.slit_width / 2;
+        // mount edges: angle 68/180 rad, thickness 5, width 6 (:338-350)
+        const double ang = 68.0 / 180.0;
+        k.a1 = 1.0 / tan(ang) - 1.0 / (sin(ang) * cos(ang));
+        k.b1 = 6.0 / cos(ang);
+        k.a2 = (cos(ang) + 1.0) / sin(ang);
+        k.b2 = -6.0;
+        k.b3 = -6.0;
+        // total-internal-reflection thresholds asin(nt / ni) of the
+        // glass-to-air surfaces (:176)
+        k.tir1 = asin(1.0 / prm.n1);
+        k.tir2 = asin(1.0 / prm.n2);
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < prm.n_z; i += blockDim.x)
+    if (tid == 0) {
+        double zlo = s_zlo[0], zhi = s_zhi[0];
+        for (int j = 1; j < kObdThreads / 32; ++j) {
+            zlo = fmin(zlo, s_zlo[j]);
+            zhi = fmax(zhi, s_zhi[j]);
+        }
+        s_k.zlo = zlo;
+        s_k.zhi = zhi;
+    }
+    __syncthreads();
+    const ScanConsts &k = s_k;
+
+    const int64_t T = kObdThreads;
+    const int64_t n_tiles = (n + T - 1) / T;
+    int64_t tile = blockIdx.x;
+    for (;;) {
+        // s_count was last written before a barrier: every thread reads the
+        // same value
+        int c = s_count;
+        while (c < T && tile < n_tiles) {
+            __syncthreads();   // all threads have read s_count before it grows
+            const int64_t i = tile * T + tid;
+            if (i < n && reaches_lens1(prm, k, p, v, w, n, i)) s_idx[atomicAdd(&s_count, 1)] = i;
+            tile += gridDim.x;
+            __syncthreads();   // the appends are complete
+            c = s_count;
+        }
+        if (c == 0) break;
+        const int take = c < T ? c : (int)T;
+        const int64_t mine = tid < take ? s_idx[c - take + tid] : -1;
+        __syncthreads();       // all reads of the queue are done
+        if (tid == 0) s_count = c - take;
+        __syncthreads();       // the shortened count is visible
+        if (mine >= 0) scan_photon(prm, k, p, v, w, n, mine, s_int);
+    }
+    __syncthreads();
+    for (int i = tid; i < prm.n_z; i += blockDim.x)
         if (s_int[i] != 0.0) atomicAdd(intensity + i, s_int[i]);
 }
 
@@ -286,15 +408,20 @@ int pmo_run_obd(const pmo_obd_params *prm, const float *p, const float *v, const
     int dev = 0;
     if (cudaGetDevice(&dev) == cudaSuccess)
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int threads = 256;
-    int64_t blocks = (n + threads - 1) / threads;
-    if (blocks > (int64_t)sms * 8) blocks = (int64_t)sms * 8;
     const size_t smem = (size_t)prm->n_z * sizeof(double);
-    if (smem > 48 * 1024 &&
+    if (smem > 40 * 1024 &&
         cudaFuncSetAttribute(obd_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem) != cudaSuccess)
         return PMO_ERR_CUDA;
-    obd_kernel<<<(unsigned)blocks, threads, smem, s>>>(*prm, p, v, w, n, intensity);
+    int occ = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, obd_kernel, kObdThreads, smem) !=
+            cudaSuccess ||
+        occ < 1)
+        return PMO_ERR_CUDA;
+    // one resident wave of blocks; each walks tiles of photons
+    int64_t blocks = (n + kObdThreads - 1) / kObdThreads;
+    if (blocks > (int64_t)sms * occ) blocks = (int64_t)sms * occ;
+    obd_kernel<<<(unsigned)blocks, kObdThreads, smem, s>>>(*prm, p, v, w, n, intensity);
     return cudaGetLastError() == cudaSuccess ? PMO_OK : PMO_ERR_CUDA;
 }
 
