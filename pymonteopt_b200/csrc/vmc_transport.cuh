@@ -363,8 +363,10 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
                 atomicAdd(kp.d_ma_voxel + lin, dma);
                 atomicAdd(kp.d_ms_voxel + lin, dms);
             }
-            atomicAdd(s_gma + lab, (double)dma);
-            atomicAdd(s_gms + lab, (double)dms);
+            if (kp.d_ma_label) {
+                atomicAdd(s_gma + lab, (double)dma);
+                atomicAdd(s_gms + lab, (double)dms);
+            }
             gL = 0.f;
             gN = 0.f;
         }

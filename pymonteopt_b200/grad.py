@@ -132,8 +132,9 @@ class _RrFunction(torch.autograd.Function):
         coef = torch.zeros(A.PMO_RR_CATS, model.nr, dtype=torch.float32, device=w.device)
         coef[A.PMO_RR_TOP] = w
         coef[A.PMO_RR_LAT_NEG] = w
+        # only the gradients this model returns are accumulated
         res = run_replay(model.dp, fwd, coef, model.seed, per_voxel=model.props == "voxel",
-                         per_label=True, precision=model.precision,
+                         per_label=model.props != "voxel", precision=model.precision,
                          block_threads=model.block_threads)
         model.last_replay = res
         if res.mismatches:

@@ -58,8 +58,16 @@ def test_replay_follows_forward(cuda, props):
     assert rep.replayed > 10000
     assert torch.isfinite(ma.grad).all() and torch.isfinite(ms.grad).all()
     if props == "voxel":
+        # the autograd path accumulates only what it returns; a replay asked
+        # for both gives per-voxel sums that add up to the per-label ones
+        assert rep.d_ma_label is None
+        coef = _coef(_weights(m.nr, R.device), m.area, m.n_photons, m.nr)
+        both = G.run_replay(m.dp, m.last_forward, coef, m.seed, per_voxel=True,
+                            per_label=True)
+        assert both.mismatches == 0
+        torch.testing.assert_close(both.d_ma_voxel, rep.d_ma_voxel, rtol=1e-5, atol=1e-9)
         lab = torch.from_numpy(prob.labels).to(cuda)
-        for d_v, d_l in ((rep.d_ma_voxel, rep.d_ma_label), (rep.d_ms_voxel, rep.d_ms_label)):
+        for d_v, d_l in ((both.d_ma_voxel, both.d_ma_label), (both.d_ms_voxel, both.d_ms_label)):
             s = d_v[lab == 0].double().sum().item()
             assert abs(s - d_l[0].item()) <= 1e-4 * abs(d_l[0].item()) + 1e-9
 
