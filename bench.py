@@ -295,6 +295,34 @@ def reference_gpu_leg(torch, dev, photons: int) -> dict:
                      "e2e_photons_per_s": photons / t_ours_e2e,
                      "Rd": float(led[A.PMO_L_RD] / photons),
                      "Tt": float(led[A.PMO_L_TT] / photons)}
+    # the drop-in entry point with the reference's own arguments and in-place
+    # state arrays (pmo_cuvmc: voxel-by-voxel stepping, no box map), timed
+    # and copied exactly as the reference kernel is above
+    ws = torch.empty(int(E.load().pmo_workspace_bytes()), dtype=torch.uint8, device=dev)
+
+    def dropin(seed):
+        E.cuvmc(*state, ref.ma, ref.ms, ref.n, ref.g, ref.model,
+                float(np.float32(prob.voxel_space)), photons, int(prob.end_label), seed, ws)
+
+    def dropin_kernel():
+        for d, s0 in zip(state, fresh):
+            d.copy_(s0)
+        dropin(7)
+    t_drop = max(timed(dropin_kernel) - t_reset, 1e-9)
+    drop_res = ref.results(*state, nr=100, dr=0.2)
+
+    def dropin_e2e():
+        for d, h in zip(state, host):
+            d.copy_(h, non_blocking=True)
+        dropin(8)
+        for h, d in zip(back, state):
+            h.copy_(d, non_blocking=True)
+    t_drop_e2e = timed(dropin_e2e)
+    out["ours_dropin_cuvmc"] = {"kernel_photons_per_s": photons / t_drop,
+                                "e2e_photons_per_s": photons / t_drop_e2e,
+                                "Rd": drop_res["Rd"], "Tt": drop_res["Tt"],
+                                "path": "pmo_cuvmc: the reference's argument list and state "
+                                        "arrays, voxel-by-voxel stepping"}
     out["speedup_kernel"] = out["ours"]["kernel_photons_per_s"] / out["reference"]["kernel_photons_per_s"]
     out["speedup_e2e"] = out["ours"]["e2e_photons_per_s"] / out["reference"]["e2e_photons_per_s"]
     return out
