@@ -5,10 +5,9 @@
 // This restates the reference's vectorised NumPy ray tracing
 // (pymopt/optics/_classes.py:50-380 for the elements, :454-526 for the
 // scan, :528-566 for the side geometry) per photon:
-// - one thread per exit photon, looping over the scan; photons that miss
-//   lens 1 at every Z are dropped by an exact-safe test first, and each
-//   block gathers the rest in a shared queue, so that a scan round gives
-//   every thread a photon that may pass;
+// - a warp per exit photon, its lanes spread over the scan's Z values;
+//   photons that miss lens 1 at every Z are dropped first by a test that
+//   cannot drop a photon the exact per-Z test would keep;
 // - the intensity of each Z summed in shared memory, then one FP64 atomic
 //   per block and Z.
 //
@@ -213,10 +212,13 @@ __device__ __forceinline__ bool reaches_lens1(const pmo_obd_params &prm, const S
     return qx * qx + qy * qy <= rm * rm;
 }
 
-// Photon i through the bench for every Z of the scan; each Z that reaches the
+// Photon i through the bench, the lanes of a warp taking every 32nd Z of
+// the scan (lane, lane + 32, ...).  Neighbouring Z send the photon along
+// nearly the same path, so the lanes pass and fail the same elements far
+// more often than 32 different photons would.  Each Z that reaches the
 // photodiode and passes the four Fresnel decisions adds w_i to s_int[Z].
 __device__ void scan_photon(const pmo_obd_params &prm, const ScanConsts &k, const float *p,
-                            const float *v, const float *w, int64_t n, int64_t i,
+                            const float *v, const float *w, int64_t n, int64_t i, int lane,
                             double *s_int) {
     const float x0 = p[i], y0 = p[n + i];
     double ux, uy, uz;
@@ -224,7 +226,8 @@ __device__ void scan_photon(const pmo_obd_params &prm, const ScanConsts &k, cons
     const double wi = (double)w[i];
     // Lens 1's flat face has the fixed normal (0, 0, -1): the incidence
     // angle, the reflectance and the refracted direction do not depend on
-    // Z, only the hit point and the draw do.  Computed once per photon,
+    // Z, only the hit point and the draw do.  The direction is computed once
+    // per photon, the reflectance the first time a Z reaches the photodiode,
     // with the same operations as inside the scan.
     Ray r1;
     r1.px = r1.py = r1.pz = 0.0;
@@ -233,9 +236,9 @@ __device__ void scan_photon(const pmo_obd_params &prm, const ScanConsts &k, cons
     r1.vz = uz;
     Cosines c1;
     refract(r1, 0.0, 0.0, -1.0, prm.n1, false, 0.0, c1);
-    const double R1 = reflectance(c1);
+    double R1 = -1.0;   // not computed yet (a computed R1 is >= 0 or NaN)
     normalize(r1);
-    for (int zi = 0; zi < prm.n_z; ++zi) {
+    for (int zi = lane; zi < prm.n_z; zi += 32) {
         const double Z = prm.z[zi];
         // element positions of this Z (:454-470)
         const double zl1 = -prm.bfl1 + Z;
@@ -289,6 +292,7 @@ __device__ void scan_photon(const pmo_obd_params &prm, const ScanConsts &k, cons
             u[2] = (double)q.z * 0x1p-32;
             u[3] = (double)q.w * 0x1p-32;
         }
+        if (R1 < 0.0) R1 = reflectance(c1);
         if (!passes(u[0], R1) || !passes(u[1], reflectance(c2)) ||
             !passes(u[2], reflectance(c3)) || !passes(u[3], reflectance(c4)))
             continue;
@@ -296,23 +300,17 @@ __device__ void scan_photon(const pmo_obd_params &prm, const ScanConsts &k, cons
     }
 }
 
-// Each block walks its tiles of kObdThreads photons, keeps the photons that
-// can reach lens 1 in a shared queue, and scans them kObdThreads at a time,
-// so that every thread of a scan round holds a photon that may pass.  (About
-// 60 % of Lambertian exits miss lens 1 at every Z of the default scan; with
-// one photon per thread their lanes would idle through all of it.)  Every
-// barrier sits in control flow that is uniform over the block: the queue
-// count is read after a barrier and the tile index is the same in all
-// threads.
-__global__ void __launch_bounds__(kObdThreads, 4) obd_kernel(pmo_obd_params prm,
+// Each warp walks tiles of 32 photons.  Its lanes test one photon each for
+// lens 1 (about 60 % of Lambertian exits miss it at every Z of the default
+// scan), then the warp scans the photons that may pass one after another,
+// its lanes spread over Z.
+__global__ void __launch_bounds__(kObdThreads, 3) obd_kernel(pmo_obd_params prm,
                                                              const float *__restrict__ p,
                                                              const float *__restrict__ v,
                                                              const float *__restrict__ w,
                                                              int64_t n,
                                                              double *__restrict__ intensity) {
     extern __shared__ double s_int[];
-    __shared__ int64_t s_idx[2 * kObdThreads];
-    __shared__ int s_count;
     __shared__ double s_zlo[kObdThreads / 32], s_zhi[kObdThreads / 32];
     __shared__ ScanConsts s_k;
     const int tid = threadIdx.x;
@@ -333,7 +331,6 @@ __global__ void __launch_bounds__(kObdThreads, 4) obd_kernel(pmo_obd_params prm,
         s_zhi[tid >> 5] = hi;
     }
     if (tid == 0) {
-        s_count = 0;
         // scan constants, read from shared memory by every thread (in
         // registers they would spill)
         ScanConsts &k = s_k;
@@ -365,28 +362,18 @@ __global__ void __launch_bounds__(kObdThreads, 4) obd_kernel(pmo_obd_params prm,
     __syncthreads();
     const ScanConsts &k = s_k;
 
-    const int64_t T = kObdThreads;
-    const int64_t n_tiles = (n + T - 1) / T;
-    int64_t tile = blockIdx.x;
-    for (;;) {
-        // s_count was last written before a barrier: every thread reads the
-        // same value
-        int c = s_count;
-        while (c < T && tile < n_tiles) {
-            __syncthreads();   // all threads have read s_count before it grows
-            const int64_t i = tile * T + tid;
-            if (i < n && reaches_lens1(prm, k, p, v, w, n, i)) s_idx[atomicAdd(&s_count, 1)] = i;
-            tile += gridDim.x;
-            __syncthreads();   // the appends are complete
-            c = s_count;
+    const int lane = tid & 31;
+    const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + tid) >> 5;
+    const int64_t n_warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t base = warp * 32; base < n; base += n_warps * 32) {   // warp-uniform
+        const int64_t i = base + lane;
+        const bool live = i < n && reaches_lens1(prm, k, p, v, w, n, i);
+        unsigned m = __ballot_sync(0xffffffffu, live);
+        while (m) {
+            const int b = __ffs(m) - 1;
+            m &= m - 1;
+            scan_photon(prm, k, p, v, w, n, base + b, lane, s_int);
         }
-        if (c == 0) break;
-        const int take = c < T ? c : (int)T;
-        const int64_t mine = tid < take ? s_idx[c - take + tid] : -1;
-        __syncthreads();       // all reads of the queue are done
-        if (tid == 0) s_count = c - take;
-        __syncthreads();       // the shortened count is visible
-        if (mine >= 0) scan_photon(prm, k, p, v, w, n, mine, s_int);
     }
     __syncthreads();
     for (int i = tid; i < prm.n_z; i += blockDim.x)
