@@ -234,7 +234,7 @@ typedef struct pmo_grad {
 #define PMO_G_COUNTERS_N 4
 
 typedef struct pmo_launch {
-    int32_t block_threads;       /* 0 = default */
+    int32_t block_threads;       /* 0 = default: 256 for pmo_run_plain, 128 for the others */
     int32_t blocks_per_sm;       /* 0 = occupancy maximum */
 } pmo_launch;
 
