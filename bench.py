@@ -550,6 +550,20 @@ def main() -> int:
             "source": "instruction counts from ncu on the same workload (profiles/vmc_plain_c2_ncu.json); "
                       "peak = 4 issue slots x SMs x median sampled SM clock",
         }
+    if traffic:
+        # the HBM side, for scale: DRAM bytes per launch (ncu, same workload)
+        # over the launch time, against the measured copy bandwidth
+        hbm_peak, hbm_src = 6650.0, "fallback (no MEASURED_PEAKS.json): 6.65 TB/s copy"
+        try:
+            with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+                mp = json.load(f)
+            if mp.get("hbm_gbs"):
+                hbm_peak, hbm_src = float(mp["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (measured)"
+        except (OSError, ValueError):
+            pass
+        gbs = traffic["dram_bytes_per_photon"] * photons / launch_s / 1e9
+        roofline["hbm"] = {"achieved": gbs, "peak": hbm_peak, "unit": "GB/s",
+                           "frac": gbs / hbm_peak, "peak_source": hbm_src}
     inflow = ledger[A.PMO_L_WINIT] + ledger[A.PMO_L_RGAIN]
     outflow = (ledger[A.PMO_L_RD] + ledger[A.PMO_L_TT] + ledger[A.PMO_L_EXIT0] +
                ledger[A.PMO_L_ABS] + ledger[A.PMO_L_RLOSS] + ledger[A.PMO_L_ERRW])
