@@ -58,6 +58,33 @@ def test_argument_validation_rejects_before_any_device_call(built_lib):
     assert built_lib.pmo_run_plain(None, None, None, None, 0, None) == A.PMO_ERR_ARG
     p = A.PmoProblem()
     assert built_lib.pmo_run_plain(C.byref(p), None, None, None, 0, None) == A.PMO_ERR_ARG
+    assert built_lib.pmo_run_grad(None, None, None, None, 0, None) == A.PMO_ERR_ARG
+    # batched slabs: the pointers are only checked for null on the host, so
+    # stand-in addresses reach the checks of the other fields
+    fake = 256
+    b = A.PmoBatch()
+    b.slabs, b.items, b.sums, b.bins = fake, fake, fake, fake
+    b.n_problems, b.n_items, b.nr, b.precision = 1, 1, 4, A.PMO_FP32
+    b.tally_mode = 7
+    assert built_lib.pmo_run_batched(C.byref(b), None, C.c_void_p(fake), 512, None) == A.PMO_ERR_ARG
+    b.tally_mode, b.precision = A.PMO_BT_GLOBAL, 5
+    assert built_lib.pmo_run_batched(C.byref(b), None, C.c_void_p(fake), 512, None) == A.PMO_ERR_ARG
+    b.precision = A.PMO_FP32
+    assert built_lib.pmo_run_batched(C.byref(b), None, None, 0, None) == A.PMO_ERR_WORKSPACE
+    # optical bench: an empty or oversized scan and a fixed draw outside [0, 1)
+    o = A.PmoObdParams()
+    o.z, o.n_z, o.fixed_u = fake, 0, -1.0
+    out = C.c_void_p(fake)
+    args = (C.c_void_p(fake), C.c_void_p(fake), C.c_void_p(fake), 10, out, None)
+    assert built_lib.pmo_run_obd(C.byref(o), *args) == A.PMO_ERR_ARG
+    o.n_z = 4097
+    assert built_lib.pmo_run_obd(C.byref(o), *args) == A.PMO_ERR_ARG
+    o.n_z, o.fixed_u = 8, 1.0
+    assert built_lib.pmo_run_obd(C.byref(o), *args) == A.PMO_ERR_ARG
+    # no photons: nothing to do, and no device call
+    o.fixed_u = -1.0
+    assert built_lib.pmo_run_obd(C.byref(o), C.c_void_p(fake), C.c_void_p(fake),
+                                 C.c_void_p(fake), 0, out, None) == A.PMO_OK
 
 
 def _c_offsets(struct_name, fields):
