@@ -289,7 +289,9 @@ def cuvmc(add: torch.Tensor, p: torch.Tensor, v: torch.Tensor, w: torch.Tensor,
 
 def main(argv=None) -> int:
     """``python -m pymonteopt_b200.engine``: time plain launches on one of the
-    synthetic volumes and print one JSON line (photons/s of the best launch)."""
+    synthetic volumes and print one JSON line (photons/s of the best launch).
+    The volume stays resident and L2 is not flushed between launches; the
+    benchmark of record is ``bench.py``."""
     import argparse
     import json
     from . import volumes as V
