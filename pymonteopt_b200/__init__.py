@@ -12,7 +12,14 @@ from .voxel import (  # noqa: E402,F401
     VoxelPlateModel,
     VoxelTuringModel,
 )
-from .turing import TuringPattern  # noqa: E402,F401
-
 __all__ = ["VoxelPlateModel", "VoxelPlateExModel", "VoxelTuringModel", "VoxelArrayModel",
            "TuringPattern"]
+
+
+def __getattr__(name):
+    # imported on first use, so that ``python -m pymonteopt_b200.turing`` runs
+    # the module once rather than over an already imported copy
+    if name == "TuringPattern":
+        from .turing import TuringPattern
+        return TuringPattern
+    raise AttributeError(f"module {__name__!r} has no attribute {name!r}")
