@@ -179,9 +179,7 @@ __global__ void __launch_bounds__(512) vmc_batched_kernel(const BParams bp) {
             bool transmit = true;
             R cb = R(1), nr = R(1);
             if (nin != nout) {
-                const uint4 fr = philox4x32_10(make_uint4(f, 1u + 4u * (uint32_t)p, j, 0u), bp.rk);
-                ++f;
-                const R u = u01<R>(fr.x);
+                const uint32_t fk = f++;   // this decision's Philox counter
                 R ca = fabs(vz);
                 if (ca > R(1)) ca = R(1);
                 nr = xdiv(nin, nout);
@@ -205,7 +203,22 @@ __global__ void __launch_bounds__(512) vmc_batched_kernel(const BParams bp) {
                         ra = xdiv(num, den);
                     }
                 }
-                transmit = ra < u;
+                // transmit when ra < u for the uniform u in (0, 1] (:150).
+                // Only 0 < ra < 1 needs u: ra == 0 always transmits, and
+                // ra >= 1 (total internal reflection, frequent at a slab's
+                // faces) or a NaN always reflects, so those skip the draw.
+                // The counter is used up either way, so later draws do not
+                // change.  Measured on C5: +2.7 % (the voxel kernel, whose
+                // Fresnel decisions run on one or two lanes, measured
+                // 0.3-1.8 % slower with the same change and keeps the draw
+                // first).
+                if (ra > R(0) && ra < R(1)) {
+                    const uint4 fr = philox4x32_10(
+                        make_uint4(fk, 1u + 4u * (uint32_t)p, j, 0u), bp.rk);
+                    transmit = ra < u01<R>(fr.x);
+                } else {
+                    transmit = ra <= R(0);
+                }
             }
             if (!transmit) {
                 vz = -vz;
