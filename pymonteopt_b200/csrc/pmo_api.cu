@@ -53,12 +53,12 @@ cudaError_t launch_normalize_fluence(const KParams &kp, int props_mode,
 }  // namespace pmo
 
 using pmo::KParams;
+using pmo::kWorkspaceBytes;
 
 namespace {
 
-constexpr size_t kWorkspaceBytes = 512;
-constexpr size_t kWsLedgerOff = 64;
-constexpr size_t kWsCountersOff = 256;
+constexpr size_t kWsLedgerOff = PMO_WS_LEDGER_OFFSET;
+constexpr size_t kWsCountersOff = PMO_WS_COUNTERS_OFFSET;
 
 bool finite_pos(float x) { return std::isfinite(x) && x > 0.f; }
 

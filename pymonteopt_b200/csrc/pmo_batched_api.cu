@@ -12,9 +12,9 @@ cudaError_t launch_batched_f64(const BParams &bp, int threads, int bps, cudaStre
 
 #include "vmc_batched.cuh"
 
-namespace {
+using pmo::kWorkspaceBytes;
 
-constexpr size_t kWorkspaceBytes = 512;
+namespace {
 
 // Rd, Tt, A, derivatives, energy residual; R(r) and its derivatives.
 __global__ void batch_finalize_kernel(const pmo_slab *__restrict__ slabs, int n_problems,

@@ -8,6 +8,16 @@
 
 namespace pmo {
 
+// Device scratch the run entry points need (pmo_workspace_bytes): the photon
+// chunk counter, and pmo_cuvmc's ledger and counters at PMO_WS_LEDGER_OFFSET
+// and PMO_WS_COUNTERS_OFFSET.
+constexpr size_t kWorkspaceBytes = 512;
+static_assert(PMO_WS_COUNTERS_OFFSET + PMO_COUNTERS_N * sizeof(unsigned long long) <=
+                  kWorkspaceBytes,
+              "pmo_cuvmc's counters must fit in the workspace");
+static_assert(kWorkspaceBytes <= PMO_STATIC_WORKSPACE_BYTES,
+              "pmo_run_plain_static must be able to provide the workspace");
+
 // Everything a transport kernel reads, passed by value (kernel parameter
 // space).  Built by the C ABI from pmo_problem / pmo_tallies.
 struct KParams {

@@ -2,23 +2,28 @@
 // arithmetic type.  Included by vmc_plain_f32.cu and vmc_plain_f64.cu, which
 // are compiled with different floating-point flags.
 #pragma once
+#include <atomic>
+
 #include "vmc_batched.cuh"
 #include "vmc_transport.cuh"
 
 namespace pmo {
 
+// SM count of the current device, cached per device ordinal.  Launches may come
+// from several host threads at once, so the cache entries are atomics (two
+// threads that miss together both query the same value).
 inline int device_sm_count() {
-    static int cached[64] = {0};
+    static std::atomic<int> cached[64];
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return 0;
     if (dev < 0 || dev >= 64) return 0;
-    if (!cached[dev]) {
-        int sms = 0;
+    int sms = cached[dev].load(std::memory_order_relaxed);
+    if (!sms) {
         if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
             return 0;
-        cached[dev] = sms;
+        cached[dev].store(sms, std::memory_order_relaxed);
     }
-    return cached[dev];
+    return sms;
 }
 
 template <typename R, int PROPS, int FLU, bool SKIP, bool GRAD = false>

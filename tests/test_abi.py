@@ -59,6 +59,12 @@ def test_argument_validation_rejects_before_any_device_call(built_lib):
     p = A.PmoProblem()
     assert built_lib.pmo_run_plain(C.byref(p), None, None, None, 0, None) == A.PMO_ERR_ARG
     assert built_lib.pmo_run_grad(None, None, None, None, 0, None) == A.PMO_ERR_ARG
+    # the entry point without a workspace argument: problem, tallies, launch, stream
+    sig = _lib.SIGNATURES["pmo_run_plain_static"]
+    assert sig == (C.c_int, [C.POINTER(A.PmoProblem), C.POINTER(A.PmoTallies),
+                             C.POINTER(A.PmoLaunch), C.c_void_p])
+    assert built_lib.pmo_run_plain_static(None, None, None, None) == A.PMO_ERR_ARG
+    assert built_lib.pmo_workspace_bytes() <= A.PMO_STATIC_WORKSPACE_BYTES
     # batched slabs: the pointers are only checked for null on the host, so
     # stand-in addresses reach the checks of the other fields
     fake = 256

@@ -23,9 +23,9 @@ from pymonteopt_b200._lib import load
 pytestmark = pytest.mark.gpu
 
 
-def _run(static: bool, dp, spec, n, seed):
+def _run(static: bool, dp, spec, n, seed, t=None):
     lib = load()
-    t = E.Tallies(dp, spec, n)
+    t = E.Tallies(dp, spec, n) if t is None else t.zero_()
     s = dp.struct(seed, 0, n, A.PMO_FP32, flags=A.PMO_FLAG_EXPORT_EXITS)
     ts = t.struct()
     launch = A.PmoLaunch(0, 0)
@@ -48,8 +48,18 @@ def test_static_workspace_entry_matches_allocating_entry(cuda):
     n, seed = 200000, 21
     spec = E.TallySpec(nr=100, dr=0.1, fluence=A.PMO_FLU_GLOBAL, export_exits=True)
     ref = _run(False, dp, spec, n, seed)
+    got = E.Tallies(dp, spec, n)        # the caller's tally buffers, allocated up front
+    _run(True, dp, spec, n, seed, got)  # the first call on the device looks up the scratch
+
+    def used():
+        torch.cuda.synchronize()
+        return torch.cuda.memory_allocated(cuda), torch.cuda.mem_get_info(cuda)[0]
+
     for _ in range(2):   # two calls in a row share the static scratch
-        got = _run(True, dp, spec, n, seed)
+        before = used()
+        _run(True, dp, spec, n, seed, got)
+        # the call allocated nothing: neither through torch nor on the device
+        assert used() == before
         # integer counters and per-photon exit states are exact; sums of
         # float atomics differ only by the order of additions
         assert np.array_equal(got.host_counters(), ref.host_counters())
