@@ -13,9 +13,13 @@
  * Photon p of a run draws all its random numbers from Philox4x32-10
  * (Salmon et al., SC'11) with key = (seed_lo, seed_hi) and counter
  * (n, stream, p_lo, p_hi): stream 0 gives the four uniforms of interaction n
- * (step length, roulette, Henyey-Greenstein cos(theta), azimuth), stream 1
- * word 0 the uniform of the n-th Fresnel decision, stream 2 the source
- * uniforms.  A photon's history therefore depends only on (seed, p, optics),
+ * (step length, a spare uniform, Henyey-Greenstein cos(theta), azimuth).  The
+ * spare uniform serves the first decision of the step that needs one more:
+ * a Fresnel decision with 0 < R < 1 during the step's face crossings, or the
+ * roulette at its end.  A later Fresnel decision of the same step takes word
+ * 0 of stream 1 at counter n = the photon's Fresnel-decision index, a later
+ * roulette word 0 of stream 3 at the interaction's index.  Stream 2 gives the
+ * source uniforms.  A photon's history therefore depends only on (seed, p, optics),
  * never on the launch shape, so runs over photon ranges can be split, resumed
  * and replayed.
  *
@@ -92,6 +96,9 @@ extern "C" {
 #define PMO_C_ERR_CAP    9
 #define PMO_C_ERR_NUM    10
 #define PMO_C_SAMECROSS  11      /* same-label crossings (counted by the oracle)  */
+#define PMO_C_XDRAWS     12      /* Philox draws beyond one per interaction: a
+                                    Fresnel decision or roulette after the step's
+                                    spare uniform was taken                      */
 #define PMO_COUNTERS_N   16
 
 /* ---- R(r) / T(r) histogram categories, layout [PMO_RR_CATS][nr] --------- */
@@ -376,8 +383,11 @@ int pmo_batch_finalize(const pmo_batch *batch, double *results, double *rr, void
  * allowed): the scratch lives in a file-scope device array of
  * PMO_STATIC_WORKSPACE_BYTES bytes that every GPU loading the library holds
  * until exit.  Returns PMO_ERR_WORKSPACE if the run needs more scratch than
- * that.  The first call on a device looks up the array's device address with
- * that device current; make that first call before any stream capture.  All
+ * that.  The first call in a CUDA context (the device's primary context, or a
+ * context the caller made current) looks up the array's device address with
+ * that context current and caches it for that context only, so a context
+ * created after cudaDeviceReset gets a fresh lookup; make that first call
+ * before any stream capture.  All
  * calls share the array: calls on one stream in sequence are fine, calls that
  * overlap on the GPU (other streams or host threads) race on it.  Allocates
  * nothing; the caller still passes the problem and the tally buffers.

@@ -136,6 +136,9 @@ static int PFX(trace)(const pmo_problem *P, const PFX(props_t) *tab,
         pmo_philox4x32_10(ctr, key, rnd);
         n_int++;
         REAL st = -LOG((REAL)pmo_u01(rnd[0]));
+        /* rnd[1] is the step's spare uniform: the first Fresnel decision with
+           0 < R < 1 in this step, or else the roulette, takes it */
+        int ry_free = 1;
 
         for (;;) {
             /* distance to the nearest voxel face, db capped at 1000 (:80-90) */
@@ -177,11 +180,6 @@ static int PFX(trace)(const pmo_problem *P, const PFX(props_t) *tab,
             if (ni != nt) {
                 /* Fresnel / total internal reflection (:105-153), written with
                    cos/sin of the incidence and transmission angles. */
-                uint32_t frn[4];
-                ctr[0] = n_fres; ctr[1] = 1; ctr[2] = idlo; ctr[3] = idhi;
-                pmo_philox4x32_10(ctr, key, frn);
-                n_fres++;
-                REAL u = (REAL)pmo_u01(frn[0]);
                 REAL ca = FABS(v[ax]);
                 if (ca > 1) ca = 1;
                 REAL ra, cb = 1;
@@ -203,7 +201,27 @@ static int PFX(trace)(const pmo_problem *P, const PFX(props_t) *tab,
                     }
                 }
                 acc->counters[PMO_C_FRESNEL]++;
-                if (ra < u) {
+                /* transmit when R < u, u uniform in (0, 1] (:150).  Only
+                   0 < R < 1 needs u: R == 0 always transmits, R >= 1 (TIR) or
+                   a NaN always reflects.  u is the spare word of the step while
+                   it is free, else word 0 of the draw (decision index, 1). */
+                int refract;
+                if (ra > 0 && ra < 1) {
+                    uint32_t word = rnd[1];
+                    if (!ry_free) {
+                        uint32_t frn[4];
+                        ctr[0] = n_fres; ctr[1] = 1; ctr[2] = idlo; ctr[3] = idhi;
+                        pmo_philox4x32_10(ctr, key, frn);
+                        word = frn[0];
+                        acc->counters[PMO_C_XDRAWS]++;
+                    }
+                    ry_free = 0;
+                    refract = ra < (REAL)pmo_u01(word);
+                } else {
+                    refract = ra <= 0;
+                }
+                n_fres++;
+                if (refract) {
                     /* refract: tangential * ni/nt, normal = sign * cos(at),
                        renormalise (:124-134) */
                     for (int a = 0; a < 3; ++a) v[a] = a == ax ? PFX(sgn)(v[a]) * cb : v[a] * nr;
@@ -278,7 +296,17 @@ static int PFX(trace)(const pmo_problem *P, const PFX(props_t) *tab,
         /* Russian roulette (:182-195) */
         if (w <= (REAL)0.0001) {
             acc->counters[PMO_C_ROULETTE]++;
-            if ((REAL)0.1 < (REAL)pmo_u01(rnd[1])) {
+            /* the spare word of the step, or word 0 of the draw (interaction
+               index, 3) when a Fresnel decision of the step took it */
+            uint32_t word = rnd[1];
+            if (!ry_free) {
+                uint32_t rrn[4];
+                ctr[0] = n_int - 1; ctr[1] = 3; ctr[2] = idlo; ctr[3] = idhi;
+                pmo_philox4x32_10(ctr, key, rrn);
+                word = rrn[0];
+                acc->counters[PMO_C_XDRAWS]++;
+            }
+            if ((REAL)0.1 < (REAL)pmo_u01(word)) {
                 acc->ledger[PMO_L_RLOSS] += (double)w;
                 w = 0;
                 for (int a = 0; a < 3; ++a) { p[a] = 0; v[a] = 0; c[a] = 0; }

@@ -60,6 +60,7 @@ PMO_C_ERR_LABEL = 8
 PMO_C_ERR_CAP = 9
 PMO_C_ERR_NUM = 10
 PMO_C_SAMECROSS = 11
+PMO_C_XDRAWS = 12
 PMO_COUNTERS_N = 16
 
 PMO_RR_TOP = 0

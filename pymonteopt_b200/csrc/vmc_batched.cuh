@@ -151,6 +151,9 @@ __global__ void __launch_bounds__(512) vmc_batched_kernel(const BParams bp) {
         const uint4 rn = philox4x32_10(make_uint4(k, 4u * (uint32_t)p, j, 0u), bp.rk);
         ++k;
         R st = pneglog(u01<R>(rn.x));
+        // rn.y is the step's spare uniform: the first Fresnel decision with
+        // 0 < ra < 1 or the roulette takes it, as in the plain kernel
+        bool ry_free = true;
         for (;;) {
             // distance to the slab face ahead (only z faces bound the slab)
             const R dzf = vz > R(0) ? xsub(th, z) : (vz < R(0) ? -z : R(0));
@@ -206,16 +209,17 @@ __global__ void __launch_bounds__(512) vmc_batched_kernel(const BParams bp) {
                 // transmit when ra < u for the uniform u in (0, 1] (:150).
                 // Only 0 < ra < 1 needs u: ra == 0 always transmits, and
                 // ra >= 1 (total internal reflection, frequent at a slab's
-                // faces) or a NaN always reflects, so those skip the draw.
-                // The counter is used up either way, so later draws do not
-                // change.  Measured on C5: +2.7 % (the voxel kernel, whose
-                // Fresnel decisions run on one or two lanes, measured
-                // 0.3-1.8 % slower with the same change and keeps the draw
-                // first).
+                // faces) or a NaN always reflects, so those take no uniform.
+                // u is the step's spare word when it is still free, else the
+                // draw (fk, 1, photon) of this decision; the decision counter
+                // advances either way.
                 if (ra > R(0) && ra < R(1)) {
-                    const uint4 fr = philox4x32_10(
-                        make_uint4(fk, 1u + 4u * (uint32_t)p, j, 0u), bp.rk);
-                    transmit = ra < u01<R>(fr.x);
+                    uint32_t word = rn.y;
+                    if (!ry_free)
+                        word = philox4x32_10(make_uint4(fk, 1u + 4u * (uint32_t)p, j, 0u),
+                                             bp.rk).x;
+                    ry_free = false;
+                    transmit = ra < u01<R>(word);
                 } else {
                     transmit = ra <= R(0);
                 }
@@ -264,7 +268,10 @@ __global__ void __launch_bounds__(512) vmc_batched_kernel(const BParams bp) {
         w = xfma(-w, ma_mt, w);
         // roulette (:182-195)
         if (w <= R(0.0001)) {
-            if (R(0.1) < u01<R>(rn.y)) {
+            uint32_t word = rn.y;
+            if (!ry_free)
+                word = philox4x32_10(make_uint4(k - 1u, 3u + 4u * (uint32_t)p, j, 0u), bp.rk).x;
+            if (R(0.1) < u01<R>(word)) {
                 add(kSlotLoss, (double)w);
                 finish();
                 return false;

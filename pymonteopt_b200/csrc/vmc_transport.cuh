@@ -257,10 +257,11 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
     R wseg = 0;
     R mt = 0, imt = 0, ma_mt = 0;   // of label lab; its index n is s_tab[lab].n
     uint32_t k = 0, f = 0, ncr = 0;
-    // the current interaction's draws, kept while its step crosses faces
+    // the current interaction's draws, kept while its step crosses faces;
+    // ry is the step's spare uniform (see cycle) and ry_free says it is unused
     uint32_t ry = 0, rz = 0, rw = 0;
     R st = 0;
-    bool pending = false;
+    bool pending = false, ry_free = false;
     // gradient replay: q of the photon, path length and sum of 1/mu_s over
     // interactions in the current cell, 1/mu_s of the cell
     float gq = 0.f, gL = 0.f, gN = 0.f, gC = 0.f;
@@ -624,6 +625,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             ry = rn.y;
             rz = rn.z;
             rw = rn.w;
+            ry_free = true;
             pending = true;
         }
         int budget = kCrossPerIter;
@@ -739,9 +741,6 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             if (ni != nt) {
                 // Fresnel / total internal reflection (:105-153) with the
                 // cosines and sines of the incidence/transmission angles
-                const uint4 fr = philox4x32_10(make_uint4(f, 1u, (uint32_t)pid, (uint32_t)(pid >> 32)), kp.rk);
-                ++f;
-                const R u = u01<R>(fr.x);
                 R ca = fabs(va);
                 if (ca > R(1)) ca = R(1);
                 const R nr = xdiv(ni, nt);
@@ -767,7 +766,26 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
                         ra = xdiv(num, den);
                     }
                 }
-                if (!(ra < u)) {
+                // transmit when ra < u for a uniform u in (0, 1] (:150).  Only
+                // 0 < ra < 1 needs u: ra == 0 always transmits; ra >= 1 (total
+                // internal reflection) or a NaN always reflects.  u is the
+                // step's spare word ry when no earlier decision of this step
+                // took it, else the draw (f, 1, photon) of this decision.
+                bool reflect;
+                if (ra > R(0) && ra < R(1)) {
+                    uint32_t word = ry;
+                    if (!ry_free) {
+                        word = philox4x32_10(make_uint4(f, 1u, (uint32_t)pid, (uint32_t)(pid >> 32)),
+                                             kp.rk).x;
+                        atomicAdd(s_cnt + PMO_C_XDRAWS, 1ull);
+                    }
+                    ry_free = false;
+                    reflect = !(ra < u01<R>(word));
+                } else {
+                    reflect = !(ra <= R(0));
+                }
+                ++f;
+                if (reflect) {
                     // reflect: stay at the face with v_axis mirrored (:150-152)
                     if (ax == 0) { vx = -vx; ivx = -ivx; }
                     else if (ax == 1) { vy = -vy; ivy = -ivy; }
@@ -808,11 +826,18 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
             if (FLU != PMO_FLU_NONE) deposit(xsub(w, wn));
             w = wn;
         }
-        // Russian roulette (:182-195)
+        // Russian roulette (:182-195): its uniform is the step's spare word,
+        // or the draw (k - 1, 3, photon) when a Fresnel decision took it
         if (w <= R(0.0001)) {
             atomicAdd(s_cnt + PMO_C_ROULETTE, 1ull);
             t_abs += (double)wseg - (double)w;
-            if (R(0.1) < u01<R>(ry)) {
+            uint32_t word = ry;
+            if (!ry_free) {
+                word = philox4x32_10(make_uint4(k - 1u, 3u, (uint32_t)pid, (uint32_t)(pid >> 32)),
+                                     kp.rk).x;
+                atomicAdd(s_cnt + PMO_C_XDRAWS, 1ull);
+            }
+            if (R(0.1) < u01<R>(word)) {
                 atomicAdd(s_led + PMO_L_RLOSS, (double)w);
                 w = wseg = R(0);
                 px = py = pz = R(0);

@@ -7,7 +7,8 @@ compare is one FP32 operation, a multiply feeding an add counts once (one
 FFMA issue), and square roots, reciprocals, logarithms and sines/cosines are
 counted separately as MUFU operations.  The integer Philox work (ten rounds of
 two 32x32 multiplies per draw) is reported beside them, not in the FP32
-numerator.
+numerator; a draw serves each interaction, and Fresnel decisions and
+roulettes mostly take the interaction's spare uniform.
 
 Event counts come from the kernel's own integer counters (interactions,
 face crossings, Fresnel evaluations, reflections, roulette draws, photons), so
@@ -61,5 +62,7 @@ def mufu_ops(counters) -> int:
 
 
 def philox_draws(counters) -> int:
-    ev = event_counts(counters)
-    return ev["interaction"] + ev["fresnel"]
+    """One draw per interaction plus the extra draws of Fresnel decisions and
+    roulettes that found the step's spare uniform taken."""
+    c = [int(x) for x in counters]
+    return c[A.PMO_C_INTERACT] + c[A.PMO_C_XDRAWS]
