@@ -50,9 +50,32 @@ def _stub_modules():
     sys.modules["pydicom.dataset"].Dataset = sys.modules["pydicom.dataset"].FileDataset = object
 
 
-# Plate cases: name -> (params, nPh, seeds, nr, dr).  'c1' is the C1 workload;
-# the others are the notebook cases of the reference (test_voxelcuda.ipynb
-# cells 5, 9, 23; test_voxcelplate.ipynb cells 6, 9) at CPU-sized counts.
+# Plate cases: name -> (params, photons per seed, seeds, nr, dr[, model kwargs[,
+# model class[, chunks per seed]]]).  'c1' is the C1 workload; 'c2_pencil' /
+# 'c2_gaussian' the C2 skin slab with a pencil and with the 1 mm 1/e^2
+# Gaussian beam the benchmark runs; the notebook cases of the reference
+# (test_voxelcuda.ipynb cells 5, 9, 23; test_voxcelplate.ipynb cells 6, 9) at
+# CPU-sized counts; and the source options of BaseVoxelMonteCarlo
+# (pymopt/voxel/_classes.py:111-203): an oblique beam and first_layer_clear on
+# the glass-covered VoxelPlateExModel.  The oblique beam with its specular part
+# as photons (initial_refrect_by_angle) is not run: the reference deletes those
+# photons from its state arrays but still passes the original nPh to the
+# kernel (pymopt/voxel/_classes.py:133-146 with :75-80), which then reads and
+# writes past the arrays' ends (glibc aborted with heap corruption here).  Its
+# expected results follow from the "oblique" case: the specular photons add
+# their fraction to Rd and fall in no R(r) bin (they are recorded at r = 0).
+#
+# A seed's photons run as `chunks` reference runs of photons/chunks each, with
+# the generators seeded per run.  The reference kernel raises
+# ZeroDivisionError on rare histories (its theta() lets cos(theta) round above
+# 1, the direction turns NaN, and Numba's fastmath zero-divisor check trips on
+# the renormalisation, pymopt/voxel/_kernel.py:12-21, :165); a run that raises
+# is recorded in "failed_runs" and replaced by the next run seed.
+C2 = dict(x_size=20.0, y_size=20.0, voxel_space=0.05, thickness=[0.1, 2.0, 17.9],
+          n=[1.4, 1.4, 1.44], n_air=1.0, ma=[0.5, 0.05, 0.01], ms=[20.0, 15.0, 10.0],
+          g=[0.8, 0.85, 0.9])
+OBLIQUE = dict(x_size=10.0, y_size=10.0, voxel_space=0.1, thickness=[2.0], n=[1.4],
+               n_air=1.0, ma=[0.1], ms=[10.0], g=[0.8])
 PLATE_CASES = {
     "c1": (dict(x_size=10.1, y_size=10.1, voxel_space=0.1, thickness=[10.0], n=[1.37],
                 n_air=1.0, ma=[0.1], ms=[10.0], g=[0.9]), 20000, 10, 100, 0.1),
@@ -64,109 +87,129 @@ PLATE_CASES = {
     "three_layer": (dict(x_size=10, y_size=10, voxel_space=0.1, thickness=[0.1, 0.1, 0.2],
                          n=[1.37, 1.37, 1.37], n_air=1.0, ma=[1.0, 1.0, 2.0],
                          ms=[100.0, 10.0, 10.0], g=[0.9, 0.0, 0.7]), 20000, 10, 100, 0.05),
-    "c2_pencil": (dict(x_size=20.0, y_size=20.0, voxel_space=0.05, thickness=[0.1, 2.0, 17.9],
-                       n=[1.4, 1.4, 1.44], n_air=1.0, ma=[0.5, 0.05, 0.01],
-                       ms=[20.0, 15.0, 10.0], g=[0.8, 0.85, 0.9]), 2000, 10, 100, 0.2),
+    "c2_pencil": (C2, 20000, 10, 100, 0.2, {}, "VoxelPlateModel", 4),
+    "c2_gaussian": (C2, 100000, 16, 100, 0.1, {"w_beam": 1.0}, "VoxelPlateModel", 10),
+    "oblique": (OBLIQUE, 20000, 10, 50, 0.1, {"beam_angle": 0.5}, "VoxelPlateModel", 8),
+    "ex_first_layer": (dict(x_size=8.0, y_size=8.0, voxel_space=0.1, thickness=[0.5, 3.0],
+                            n=[1.5, 1.33], n_air=1.0, ma=[1e-5, 0.05], ms=[1e-5, 5.0],
+                            g=[0.9, 0.8]), 20000, 10, 50, 0.1, {}, "VoxelPlateExModel", 4),
 }
 
 
-def _radial(p, w, nn, dr, nph, metrics):
-    _, r = metrics.radialDistance(p, w, nn, dr, nph)
-    return r
-
-
 def run_plate_case(ref_root: str, name: str) -> dict:
-    _stub_modules()
-    sys.path.insert(0, ref_root)
-    from numba import njit
-    from pymopt import metrics
-    from pymopt.voxel import VoxelPlateModel
-
-    @njit
-    def _seed(s):
-        np.random.seed(s)
-
-    params, nph, seeds, nr, dr = PLATE_CASES[name]
-    out = {"case": name, "params": params, "nPh": nph, "seeds": list(range(seeds)),
+    """Per-seed Rd / Tt / R(r) / T(r) of the reference's own model class
+    (oracle/ref_cpu.py runs it on spawned processes)."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import ref_cpu
+    case = PLATE_CASES[name]
+    params, nph, seeds, nr, dr = case[:5]
+    model_kwargs = case[5] if len(case) > 5 else {}
+    model_class = case[6] if len(case) > 6 else "VoxelPlateModel"
+    chunks = case[7] if len(case) > 7 else 1
+    per_run = nph // chunks
+    need = seeds * chunks
+    done, failed, nxt = [], [], 0
+    while len(done) < need:
+        batch = list(range(nxt, nxt + need - len(done)))
+        nxt = batch[-1] + 1
+        runs = ref_cpu.run_plate_seeds(params, per_run, batch, model_kwargs, nr, dr,
+                                       path=ref_root, model_class=model_class)
+        for s, r in zip(batch, runs):
+            (failed.append(s) if r is None else done.append(r))
+    out = {"case": name, "params": params, "nPh": per_run * chunks, "seeds": list(range(seeds)),
+           "model_class": model_class, "model_kwargs": model_kwargs, "runs_per_seed": chunks,
+           "run_seeds": [], "failed_runs": failed,
            "nr": nr, "dr": dr, "Rd": [], "Tt": [], "Rr": [], "Tr": [], "seconds": []}
-    for s in range(seeds):
-        model = VoxelPlateModel(nPh=nph)
-        with contextlib.redirect_stdout(io.StringIO()):
-            model.build(**params)
-            _seed(s)
-            t0 = time.time()
-            model.start()
-            out["seconds"].append(time.time() - t0)
-        res = model.get_result()
-        v, w, p = res["v"], res["w"], res["p"]
-        rd = v[2] < 0
-        tt = v[2] > 0
-        out["Rd"].append(float(w[rd].sum() / nph))
-        out["Tt"].append(float(w[tt].sum() / nph))
-        out["Rr"].append(_radial(p[:, rd], w[rd], nr, dr, nph, metrics).tolist())
-        out["Tr"].append(_radial(p[:, tt], w[tt], nr, dr, nph, metrics).tolist())
+    for i in range(seeds):
+        part = done[i * chunks:(i + 1) * chunks]
+        out["run_seeds"].append([r["seed"] for r in part])
+        out["seconds"].append(sum(r["seconds"] for r in part))
+        for k in ("Rd", "Tt"):
+            out[k].append(float(np.mean([r[k] for r in part])))
+        for k in ("Rr", "Tr"):
+            out[k].append(np.mean([r[k] for r in part], axis=0).tolist())
     return out
 
 
-def run_c3_case(ref_root: str, nph: int = 2000, seeds: int = 10, nr: int = 100,
-                dr: float = 0.2) -> dict:
-    """C3 through the reference kernel directly: there is no reference model
-    class for a raw label volume, so ``vmc_kernel`` is called on the padded
-    volume with the state the reference's start() would build
-    (pymopt/voxel/_classes.py:63-81)."""
-    _stub_modules()
-    sys.path.insert(0, ref_root)
+def _c3_chunk(args):
+    """One chunk of C3 photons through the reference's ``vmc_kernel`` with
+    Numba's generator seeded by ``chunk``; None when the kernel raises."""
+    ref_root, chunk, nph, nr, dr = args
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
     sys.path.insert(0, REPO)
-    from numba import njit
+    import ref_cpu
+    from pymonteopt_b200.volumes import c3_ct_like
+    ref_cpu.stub_modules()
+    if ref_root not in sys.path:
+        sys.path.insert(0, ref_root)
     from pymopt import metrics
     from pymopt.voxel import vmc_kernel
-    from pymonteopt_b200.volumes import c3_ct_like
-
-    @njit
-    def _seed(s):
-        np.random.seed(s)
-
     prob = c3_ct_like(0)
     vol = prob.labels.astype(np.int8)
     end = prob.end_label
     cx, cy = prob.center
-    out = {"case": "c3", "volume_seed": 0, "nPh": nph, "seeds": [], "failed_seeds": [],
-           "nr": nr, "dr": dr, "Rd": [], "Tt": [], "Rr": [], "Tr": [], "seconds": []}
     l = prob.voxel_space
-    s = -1
-    while len(out["seeds"]) < seeds:
-        s += 1
-        add = np.zeros((3, nph), np.int32)
-        add[0], add[1], add[2] = cx, cy, 1
-        p = np.zeros((3, nph), np.float32)
-        p[2] = -l / 2
-        v = np.zeros((3, nph), np.float32)
-        v[2] = 1
-        w = np.full(nph, prob.src_w0, np.float32)
-        _seed(s)
-        t0 = time.time()
-        try:
-            with contextlib.redirect_stdout(io.StringIO()):
-                add, p, v, w = vmc_kernel(add, p, v, w, prob.ma[:end].copy(),
-                                          prob.ms[:end].copy(), prob.n.copy(),
-                                          prob.g[:end].copy(), vol, l, np.int32(nph),
-                                          np.int8(end))
-        except ZeroDivisionError:
-            # the reference kernel divides by zero on some histories of this
-            # heterogeneous volume (Numba's Python error model raises); such
-            # seeds are recorded and skipped
-            out["failed_seeds"].append(s)
-            continue
-        out["seeds"].append(s)
-        out["seconds"].append(time.time() - t0)
-        enc = p.astype(np.float64).copy()
-        enc[0] = l * (add[0] - cx) + p[0]
-        enc[1] = l * (add[1] - cy) + p[1]
-        rd, tt = v[2] < 0, v[2] > 0
-        out["Rd"].append(float(w[rd].sum() / nph))
-        out["Tt"].append(float(w[tt].sum() / nph))
-        out["Rr"].append(_radial(enc[:, rd], w[rd], nr, dr, nph, metrics).tolist())
-        out["Tr"].append(_radial(enc[:, tt], w[tt], nr, dr, nph, metrics).tolist())
+    add = np.zeros((3, nph), np.int32)
+    add[0], add[1], add[2] = cx, cy, 1
+    p = np.zeros((3, nph), np.float32)
+    p[2] = -l / 2
+    v = np.zeros((3, nph), np.float32)
+    v[2] = 1
+    w = np.full(nph, prob.src_w0, np.float32)
+    ref_cpu.seed_all(chunk)
+    t0 = time.time()
+    try:
+        with contextlib.redirect_stdout(io.StringIO()):
+            add, p, v, w = vmc_kernel(add, p, v, w, prob.ma[:end].copy(), prob.ms[:end].copy(),
+                                      prob.n.copy(), prob.g[:end].copy(), vol, l,
+                                      np.int32(nph), np.int8(end))
+    except ZeroDivisionError:
+        return None
+    dt = time.time() - t0
+    enc = p.astype(np.float64).copy()
+    enc[0] = l * (add[0] - cx) + p[0]
+    enc[1] = l * (add[1] - cy) + p[1]
+    rd, tt = v[2] < 0, v[2] > 0
+    return {"chunk": chunk, "seconds": dt, "w_rd": float(w[rd].sum()), "w_tt": float(w[tt].sum()),
+            "rr": metrics.radialDistance(enc[:, rd], w[rd], nr, dr, nph)[1] * nph,
+            "tr": metrics.radialDistance(enc[:, tt], w[tt], nr, dr, nph)[1] * nph}
+
+
+def run_c3_case(ref_root: str, nph: int = 2000, chunks_per_seed: int = 10, seeds: int = 10,
+                nr: int = 100, dr: float = 0.2) -> dict:
+    """C3 through the reference kernel directly: there is no reference model
+    class for a raw label volume, so ``vmc_kernel`` is called on the padded
+    volume with the state the reference's start() would build
+    (pymopt/voxel/_classes.py:63-81).
+
+    The reference kernel raises ZeroDivisionError on rare histories of this
+    volume (Numba's Python error model), so photons run in chunks of ``nph``
+    with Numba's generator seeded per chunk; a chunk that raises is recorded
+    and skipped, and each fixture seed is the sum of ``chunks_per_seed``
+    chunks that completed."""
+    import multiprocessing as mp
+    need = chunks_per_seed * seeds
+    done, failed, nxt = [], [], 0
+    with mp.get_context("spawn").Pool(os.cpu_count() or 1) as pool:
+        while len(done) < need:
+            batch = list(range(nxt, nxt + (need - len(done)) + 4))
+            nxt = batch[-1] + 1
+            for c, r in zip(batch, pool.map(_c3_chunk, [(ref_root, c, nph, nr, dr) for c in batch])):
+                (failed.append(c) if r is None else done.append(r))
+    done = sorted(done, key=lambda r: r["chunk"])[:need]
+    n_seed = nph * chunks_per_seed
+    out = {"case": "c3", "volume_seed": 0, "nPh": n_seed, "chunk_photons": nph,
+           "seeds": [], "chunks": [], "failed_chunks": failed,
+           "nr": nr, "dr": dr, "Rd": [], "Tt": [], "Rr": [], "Tr": [], "seconds": []}
+    for i in range(seeds):
+        part = done[i * chunks_per_seed:(i + 1) * chunks_per_seed]
+        out["seeds"].append(i)
+        out["chunks"].append([r["chunk"] for r in part])
+        out["seconds"].append(sum(r["seconds"] for r in part))
+        out["Rd"].append(sum(r["w_rd"] for r in part) / n_seed)
+        out["Tt"].append(sum(r["w_tt"] for r in part) / n_seed)
+        out["Rr"].append((sum(r["rr"] for r in part) / n_seed).tolist())
+        out["Tr"].append((sum(r["tr"] for r in part) / n_seed).tolist())
     return out
 
 

@@ -288,7 +288,7 @@ def test_fp32_statistics_match_reference(cuda, case):
         prob = V.c2_skin(gaussian=False)
     else:
         prob = V.plate_problem(g["params"])
-    n_per = 100000 if case != "c2_pencil" else 20000
+    n_per = 100000
     Rd, Tt, Rr, Tr = _gpu_seed_batches(prob, range(100, 110), n_per, cuda, g["nr"], g["dr"])
     for mine, ref in ((Rd, g["Rd"]), (Tt, g["Tt"])):
         m, s = mean_se(mine)
