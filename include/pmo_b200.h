@@ -451,21 +451,26 @@ typedef struct pmo_obd_params {
 int pmo_run_obd(const pmo_obd_params *prm, const float *p, const float *v, const float *w, int64_t n,
             double *intensity, void *stream);
 
-/* Philox4x32-10 words of the engine's generator for n counters ctr[4*n]
+/* ---- test and benchmark hooks ------------------------------------------
+   The three entry points below serve the test-suite and bench.py only (the
+   random-stream known-answer checks and the measured denominator of the
+   roofline); no transport path calls them. */
+
+/* Test hook.  Philox4x32-10 words of the engine's generator for n counters ctr[4*n]
    (device arrays) under key (key0, key1): known-answer checks of the random
    stream layout.  No counterpart in the reference (it uses cuRAND XORWOW,
    pymopt/voxel_gpu/_cukernel.py:42-43). */
 int pmo_philox_words(const uint32_t *ctr, uint32_t key0, uint32_t key1,
                      uint32_t *out, int n, void *stream);
 
-/* cuRAND's Philox4_32_10 for comparison: words of curand4() after
+/* Test hook.  cuRAND's Philox4_32_10 for comparison: words of curand4() after
    curand_init(seed, subsequence[i], 4 * block[i]). */
 int pmo_philox_words_curand(unsigned long long seed,
                             const unsigned long long *subsequence,
                             const unsigned long long *block, uint32_t *out,
                             int n, void *stream);
 
-/* FP32 issue-rate probe: blocks x threads threads each issue iters * 128
+/* Benchmark hook.  FP32 issue-rate probe: blocks x threads threads each issue iters * 128
    independent FFMA instructions.  Timed by the caller; gives the measured
    denominator of the FP32-issue roofline.  No counterpart in the reference. */
 int pmo_fp32_probe(float *out, int blocks, int threads, int iters, void *stream);

@@ -31,8 +31,19 @@ OUT_DIR = os.path.join(HERE, "_ref")
 LIB = os.path.join(OUT_DIR, "libcuvmc_ref.so")
 KERNEL_CU = os.path.join(OUT_DIR, "cuvmc_reference.cu")
 LAUNCHER = os.path.join(HERE, "ref_gpu_launch.cu")
-REFERENCE_ROOT = os.environ.get("PMO_REFERENCE_ROOT", "/root/reference")
 KERNEL_PY = os.path.join("pymopt", "voxel_gpu", "_cukernel.py")
+
+
+def default_reference_root() -> str | None:
+    """A pyMonteOpt checkout named by ``PMO_REFERENCE_ROOT``, else a checkout
+    called ``reference`` beside this repository, else None (nothing to build;
+    a library built earlier is kept)."""
+    repo = os.path.dirname(HERE)
+    for cand in (os.environ.get("PMO_REFERENCE_ROOT"),
+                 os.path.join(os.path.dirname(repo), "reference")):
+        if cand and os.path.exists(os.path.join(cand, KERNEL_PY)):
+            return cand
+    return None
 
 
 def _nvcc() -> str:
@@ -42,7 +53,7 @@ def _nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
-def extract(reference_root: str = REFERENCE_ROOT) -> str:
+def extract(reference_root: str) -> str:
     """The CUDA source string of ``cp.RawKernel(r\"\"\"...\"\"\", "cuVMC")``."""
     with open(os.path.join(reference_root, KERNEL_PY), encoding="utf-8") as f:
         text = f.read()
@@ -56,9 +67,12 @@ def available() -> bool:
     return os.path.exists(LIB)
 
 
-def build(force: bool = False, reference_root: str = REFERENCE_ROOT) -> str | None:
-    """Build ``libcuvmc_ref.so``; None when the reference tree is absent and
-    no library was built before."""
+def build(force: bool = False, reference_root: str | None = None) -> str | None:
+    """Build ``libcuvmc_ref.so``; None when no reference checkout is given or
+    found and no library was built before."""
+    reference_root = reference_root or default_reference_root()
+    if reference_root is None:
+        return LIB if available() else None
     src = os.path.join(reference_root, KERNEL_PY)
     if not os.path.exists(src):
         return LIB if available() else None
@@ -81,4 +95,5 @@ def build(force: bool = False, reference_root: str = REFERENCE_ROOT) -> str | No
 
 
 if __name__ == "__main__":
-    print(build(force="--force" in sys.argv))
+    args = [a for a in sys.argv[1:] if not a.startswith("--")]
+    print(build(force="--force" in sys.argv, reference_root=args[0] if args else None))

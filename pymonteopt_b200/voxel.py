@@ -30,7 +30,7 @@ import numpy as np
 
 from . import _abi as A
 from .problem import TransportProblem, center_add
-from .utils import ToJsonEncoder, _deprecate_positional_args, calTime, set_params
+from .utils import ToJsonEncoder, calTime, set_params
 
 __all__ = ["VoxelPlateModel", "VoxelPlateExModel", "VoxelTuringModel", "VoxelArrayModel",
            "PlateModel", "PlateExModel", "TuringModel_Rectangular", "TuringModel_Cylinder",
@@ -57,7 +57,6 @@ class VoxelModel:
 class PlateModel(VoxelModel):
     """Layered slab (pymopt/voxel_gpu/_classes.py:396-468)."""
 
-    @_deprecate_positional_args
     def __init__(self):
         self.model_name = "PlateModel"
         self.dtype_f = np.float32
@@ -434,7 +433,7 @@ class BaseVoxelMonteCarlo(metaclass=ABCMeta):
     @abstractmethod
     def __init__(self, *, nPh, model, dtype_f=np.float32, dtype=np.int32,
                  beam_type="TEM00", w_beam=0, beam_angle=0, initial_refrect_by_angle=False,
-                 first_layer_clear=False, threadnum=128, nr=100, dr=0.1, fluence=False,
+                 first_layer_clear=False, threadnum=None, nr=100, dr=0.1, fluence=False,
                  n_ang=0, n_line=0, line_dr=0.1, line_y_range=5.0,
                  keep_exits=None, precision="fp32", verbose=True, device=None):
         def __check_list_name(name, name_list):
@@ -453,9 +452,11 @@ class BaseVoxelMonteCarlo(metaclass=ABCMeta):
         self.beam_angle = beam_angle
         self.model = model
         self.first_layer_clear = first_layer_clear
-        if threadnum > 1024:
+        # threads per block as in the reference (pymopt/voxel_gpu/_classes.py:70-73);
+        # None leaves the launch shape to the engine (its tuned default)
+        if threadnum is not None and threadnum > 1024:
             raise Exception("There are too many threads. threadnum < 1024.")
-        self.threadnum = int(threadnum)
+        self.threadnum = None if threadnum is None else int(threadnum)
         self.nr = int(nr)
         self.dr = float(dr)
         self.n_ang = int(n_ang)
@@ -472,6 +473,7 @@ class BaseVoxelMonteCarlo(metaclass=ABCMeta):
         self.device = device
         self._dprob = None
         self._dprob_key = None
+        self._labels_at_upload = None
         self._tallies = None
         self.Rdw = self.Ttw = None
         self._reset_results()
@@ -538,8 +540,11 @@ class BaseVoxelMonteCarlo(metaclass=ABCMeta):
         vm = np.asarray(m.voxel_model)
         n = np.asarray(m.n, np.float32)
         end = int(m.end_point)
+        # the reference's int8 labels reinterpreted as uint8 (the same bytes
+        # as astype for every value) without copying the volume
+        labels = vm.view(np.uint8) if vm.dtype == np.int8 else vm.astype(np.uint8)
         prob = TransportProblem(
-            labels=vm.astype(np.uint8), voxel_space=float(m.voxel_space), end_label=end,
+            labels=labels, voxel_space=float(m.voxel_space), end_label=end,
             ma=m.ma, ms=m.ms, g=m.g, n=n,
             center=(self._get_center_add(vm.shape[0]), self._get_center_add(vm.shape[1])),
             vox_ma=getattr(m, "vox_ma", None), vox_ms=getattr(m, "vox_ms", None),
@@ -548,14 +553,19 @@ class BaseVoxelMonteCarlo(metaclass=ABCMeta):
 
     # ---- run ---------------------------------------------------------------
     def _device_problem(self):
+        """The resident volume of this model, uploaded again (with its box
+        map) whenever the model was rebuilt or its labels or optics changed.
+        The label volume is snapshotted at upload, so an in-place edit of
+        ``model.voxel_model`` between two starts is seen too."""
         from . import engine as E
         prob = self.transport_problem()
         key = (id(self.model.voxel_model), prob.labels.shape, prob.ma.tobytes(),
                prob.ms.tobytes(), prob.g.tobytes(), prob.n.tobytes())
         if self._dprob is None or self._dprob_key != key or \
-                not np.array_equal(self._dprob.host.labels, prob.labels):
+                not np.array_equal(self._labels_at_upload, prob.labels):
             self._dprob = E.DeviceProblem(prob, self.device)
             self._dprob_key = key
+            self._labels_at_upload = prob.labels.copy()
         else:
             self._dprob.host = prob  # source may have changed (beam settings)
         return self._dprob
@@ -578,7 +588,7 @@ class BaseVoxelMonteCarlo(metaclass=ABCMeta):
             print("")
         start_ = time.time()
         tal = E.Tallies(dp, spec, self.nPh)
-        bt = max(32, min(512, 32 * round(self.threadnum / 32)))
+        bt = 0 if self.threadnum is None else max(32, min(512, 32 * round(self.threadnum / 32)))
         E.run_plain(dp, self.nPh, int(rand_seed), tallies=tal,
                     precision=A.PMO_FP64 if self.precision == "fp64" else A.PMO_FP32,
                     block_threads=bt)
@@ -805,7 +815,7 @@ class BaseVoxelMonteCarlo(metaclass=ABCMeta):
 class VoxelPlateModel(BaseVoxelMonteCarlo):
     def __init__(self, *, nPh=1000, dtype_f=np.float32, dtype=np.int32, beam_type="TEM00",
                  w_beam=0, beam_angle=0, initial_refrect_by_angle=False, first_layer_clear=False,
-                 threadnum=128, **kw):
+                 threadnum=None, **kw):
         super().__init__(nPh=nPh, model=PlateModel(), dtype_f=dtype_f, dtype=dtype,
                          w_beam=w_beam, beam_angle=beam_angle, beam_type=beam_type,
                          initial_refrect_by_angle=initial_refrect_by_angle,
@@ -815,7 +825,7 @@ class VoxelPlateModel(BaseVoxelMonteCarlo):
 class VoxelPlateExModel(BaseVoxelMonteCarlo):
     def __init__(self, *, nPh=1000, dtype_f=np.float32, dtype=np.int32, beam_type="TEM00",
                  w_beam=0, beam_angle=0, initial_refrect_by_angle=False, first_layer_clear=True,
-                 threadnum=128, **kw):
+                 threadnum=None, **kw):
         super().__init__(nPh=nPh, model=PlateExModel(), dtype_f=dtype_f, dtype=dtype,
                          w_beam=w_beam, beam_angle=beam_angle, beam_type=beam_type,
                          initial_refrect_by_angle=initial_refrect_by_angle,
@@ -834,7 +844,7 @@ class VoxelPlateExModel(BaseVoxelMonteCarlo):
 class VoxelTuringModel(BaseVoxelMonteCarlo):
     def __init__(self, *, nPh=1000, dtype_f=np.float32, dtype=np.int32, beam_type="TEM00",
                  w_beam=0, beam_angle=0, initial_refrect_by_angle=False, first_layer_clear=False,
-                 threadnum=128, model_name="TuringModel", **kw):
+                 threadnum=None, model_name="TuringModel", **kw):
         self.namelist = ["TuringModel_Rectangular", "TuringModel_Cylinder", "TuringModel_RnC"]
         if model_name == self.namelist[0]:
             model = TuringModel_Rectangular()

@@ -164,11 +164,11 @@ def test_reference_kernel_library_builds_and_exports():
         import ref_gpu_build
     finally:
         sys.path.pop(0)
-    kernel_py = os.path.join(ref_gpu_build.REFERENCE_ROOT, ref_gpu_build.KERNEL_PY)
-    if os.path.exists(kernel_py):
-        src = ref_gpu_build.extract()
+    root = ref_gpu_build.default_reference_root()
+    if root is not None:
+        src = ref_gpu_build.extract(root)
         assert "__global__ void cuVMC(" in src and "curand_init" in src
-        ref_gpu_build.build()
+        ref_gpu_build.build(reference_root=root)
     if not ref_gpu_build.available():
         pytest.skip("reference tree absent and no prebuilt reference kernel")
     lib = ctypes.CDLL(ref_gpu_build.LIB)
