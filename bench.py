@@ -9,10 +9,13 @@ dataset is involved.
 
 ``value`` is photons/s with the volume resident in HBM, timed with CUDA events
 on the launching stream, L2 flushed between steps; ``e2e`` is the same metric
-through the engine API with the label volume copied from pinned host memory
-and the tallies read back every step.  ``--impl reference`` times the CPU
-restatement of the reference algorithm (oracle/vmc_oracle.c, FP32, all host
-threads) on a bounded sample of the same workload.
+through the drop-in model API, every step: ``VoxelPlateModel.build`` on the
+host, ``start`` (label and table upload, box map, transport, ledger read)
+and the Rd/Tt and R(r) getters.  ``parity`` holds the timed run against the
+reference's own runs of the workload (tests/golden/ref_c2_gaussian.json).
+``--impl reference`` and ``cpu_baseline`` time the reference's own CPU path
+(pymopt.voxel, Numba, unmodified, from baseline/_ref) on all host cores, on
+bounded samples of the same workload.
 
 Multi-GPU (``torchrun --nproc-per-node N``): photons are independent, so each
 rank runs its own photon range of the same problem (weak scaling, no
@@ -143,8 +146,9 @@ def host_threads() -> int:
 
 
 def cpu_oracle_rate(target_seconds: float, seed: int = 1234) -> dict:
-    """Photons/s of the FP32 CPU restatement on this host's cores, on a
-    bounded sample of the benchmark workload."""
+    """Photons/s of the FP32 C restatement (oracle/vmc_oracle.c, OpenMP on
+    all host threads) on a bounded sample of the benchmark workload: context
+    for the reference's own CPU path, which runs one photon at a time."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle  # noqa: E402  (test infrastructure; CPU baseline only)
     from pymonteopt_b200 import _abi as A
@@ -165,34 +169,127 @@ def cpu_oracle_rate(target_seconds: float, seed: int = 1234) -> dict:
             "Rd": float(r["ledger"][A.PMO_L_RD] / n2)}
 
 
+class ReferenceCPU:
+    """The reference's own CPU path on this host: ``VoxelPlateModel(nPh,
+    w_beam=1.0).build(**C2).start()`` (Numba ``vmc_kernel``,
+    pymopt/voxel/_kernel.py:23-172, one photon after another), unmodified,
+    imported from the copy in baseline/_ref (oracle/ref_cpu.py).  ``processes``
+    independent spawned processes with distinct seeds; Numba's JIT runs before
+    the first timed sample.  A step times every process's own start() on
+    ``n_per`` photons; its rate is all photons over the slowest process."""
+
+    def __init__(self, processes: int):
+        sys.path.insert(0, os.path.join(REPO, "oracle"))
+        import ref_cpu  # noqa: E402  (reference baseline only)
+        from pymonteopt_b200 import volumes as V
+        self.ref_cpu = ref_cpu
+        if not ref_cpu.available():
+            raise RuntimeError("baseline/_ref holds no copy of the reference "
+                               "(python oracle/ref_cpu.py <reference checkout>)")
+        import numba  # noqa: F401  (the reference's kernel needs it)
+        self.processes = processes
+        self.pool = ref_cpu.RefPool(dict(V.C2_PARAMS), processes, {"w_beam": V.C2_W_BEAM})
+        self.rate_per_process = None
+
+    def calibrate(self, photons: int = 1000, seed: int = 50) -> dict:
+        r = self.pool.step(photons, seed)
+        self.rate_per_process = photons / max(r["seconds"], 1e-6)
+        return r
+
+    def timed(self, seconds: float, seed: int) -> dict:
+        n_per = int(min(2e6, max(1000, self.rate_per_process * seconds)))
+        return self.pool.step(n_per, seed)
+
+    def close(self):
+        self.pool.close()
+
+    def describe(self) -> dict:
+        return {"cpu": self.ref_cpu.host_cpu(), "processes": self.processes,
+                "code": "reference pymopt.voxel VoxelPlateModel.start (Numba vmc_kernel), "
+                        "unmodified copy in baseline/_ref, one photon at a time per process"}
+
+
+def reference_cpu_baseline(target_seconds: float = 8.0) -> dict:
+    """cpu_baseline of this arm: the reference's own CPU path on all host
+    cores, one bounded sample of the workload, plus one process alone."""
+    threads = host_threads()
+    ref = ReferenceCPU(threads)
+    try:
+        ref.calibrate()
+        r = ref.timed(target_seconds, seed=60)
+        desc = ref.describe()
+    finally:
+        ref.close()
+    one = ReferenceCPU(1)
+    try:
+        one.calibrate()
+        r1 = one.timed(target_seconds / 2, seed=70)
+    finally:
+        one.close()
+    return {"value": r["value"], "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"{r['photons']} photons of the workload ({r['photons'] // threads} per "
+                      f"process) in {r['seconds']:.1f} s on {threads} processes; "
+                      f"one process alone: {r1['value']:.4g} photons/s "
+                      f"({r1['photons']} photons in {r1['seconds']:.1f} s)",
+            "single_process_value": r1["value"], **desc}
+
+
 def run_reference(args, rank: int, world: int) -> None:
-    """Reference arm: the CPU restatement of the reference transport
-    (oracle/vmc_oracle.c, FP32, all host threads) on a bounded sample of the
-    workload per step.  Under torchrun only rank 0 runs."""
+    """Reference arm: the reference's own CPU path (ReferenceCPU) on all host
+    cores; each step is a bounded sample of the workload (its photons and
+    seconds are the step's own).  Falls back to the C restatement, marked
+    kind "port", only if the reference copy or Numba is missing.  Under
+    torchrun only rank 0 runs."""
     if rank != 0:
         return
     photons = int(args.photons)
-    per_step = max(2.0, min(20.0, 150.0 / max(args.steps + args.warmup, 1)))
-    for _ in range(args.warmup):
-        cpu_oracle_rate(per_step / 4)
-    vals, secs, sample = [], 0.0, 0
-    for k in range(args.steps):
-        r = cpu_oracle_rate(per_step, seed=100 + k)
-        vals.append(r["value"])
-        secs += r["seconds"]
-        sample += r["photons"]
-    value = float(np.mean(vals))
+    threads = host_threads()
+    per_step = max(1.0, min(8.0, 120.0 / max(args.steps, 1)))
+    vals, secs, sample = [], [], 0
+    try:
+        ref = ReferenceCPU(threads)
+    except (RuntimeError, ImportError) as e:
+        ref, why = None, str(e)
+    if ref is not None:
+        try:
+            for k in range(max(args.warmup, 1)):
+                ref.calibrate(seed=80 + k)
+            for k in range(args.steps):
+                r = ref.timed(per_step, seed=100 + k)
+                vals.append(r["value"])
+                secs.append(r["seconds"])
+                sample += r["photons"]
+            desc = ref.describe()
+        finally:
+            ref.close()
+        kind = "reference"
+        what = (f"{sample} photons of the workload over {args.steps} steps "
+                f"({sum(secs):.1f} s of start() time, {threads} processes)")
+    else:
+        for _ in range(args.warmup):
+            cpu_oracle_rate(per_step / 4)
+        for k in range(args.steps):
+            r = cpu_oracle_rate(per_step, seed=100 + k)
+            vals.append(r["value"])
+            secs.append(r["seconds"])
+            sample += r["photons"]
+        kind, desc = "port", {"reference_unavailable": why}
+        what = (f"{sample} photons of the workload over {args.steps} steps "
+                f"({sum(secs):.1f} s), oracle/vmc_oracle.c FP32, OpenMP")
+    value = float(sample / sum(secs))
     line = {
         "impl": "reference",
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * photons / value,
+        "ms_per_step": 1e3 * float(np.mean(secs)),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "fp32", "data": "synthetic",
         "config": config_dict(photons, world),
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": r["threads"], "kind": "port",
-                         "sample": f"{sample} photons of the workload over {args.steps} steps "
-                                   f"({secs:.1f} s), oracle/vmc_oracle.c FP32, OpenMP"},
+        "step_sample": {"photons_per_step": sample // max(args.steps, 1),
+                        "note": "each step runs this many photons of the workload; "
+                                "ms_per_step is that sample's own time"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                         "sample": what, **desc},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -368,12 +465,15 @@ def gradient_leg(torch, dev, photons: int = 10_000_000, evals: int = 3) -> dict:
 def precision_leg(torch, dev, photons: int = 1_000_000) -> dict:
     """Error of the FP32 product against the FP64 build of the same kernel on
     identical Philox streams (the per-photon oracle): Rd, Tt, A, R(r) and the
-    absorbed grid, on C1 (with the fluence tally) and on this workload (C2)."""
+    absorbed grid, on C1 and on the CT-like volume (both with the fluence
+    tally; the CT-like volume has the most Fresnel events per photon) and on
+    this workload (C2)."""
     from pymonteopt_b200 import _abi as A
     from pymonteopt_b200 import engine as E
     from pymonteopt_b200 import volumes as V
     out = {"photons": photons}
     for name, prob, flu in (("c1_slab", V.c1_slab(), A.PMO_FLU_GLOBAL),
+                            ("c3_ct_like", V.c3_ct_like(0), A.PMO_FLU_GLOBAL),
                             ("c2_skin", V.c2_skin(), A.PMO_FLU_NONE)):
         dp = E.DeviceProblem(prob, dev)
         runs = {}
@@ -405,6 +505,64 @@ def precision_leg(torch, dev, photons: int = 1_000_000) -> dict:
                 "max_rel_err_hot_voxels": float(((g32 - g64).abs()[hot] / g64[hot]).max()),
                 "hot_voxels": int(hot.sum())}
         out[name] = r
+    return out
+
+
+def parity_vs_reference(tallies, photons: int) -> dict:
+    """The timed run against the reference's own VoxelPlateModel(w_beam=1.0)
+    runs of the same workload (tests/golden/ref_c2_gaussian.json, made by
+    tests/golden/make_golden.py): z-scores of Rd and Tt and per-bin z of R(r)
+    and T(r), each timed step one sample.  The fixture's standard error
+    dominates (1.6e6 reference photons against 1e8 per step)."""
+    from scipy import stats as st
+    from pymonteopt_b200 import _abi as A
+    path = os.path.join(REPO, "tests", "golden", "ref_c2_gaussian.json")
+    with open(path) as f:
+        g = json.load(f)
+    nr, dr = g["nr"], g["dr"]
+    area = np.array([2 * np.pi * (i + 0.5) * dr ** 2 for i in range(nr)])
+    Rd, Tt, Rr, Tr = [], [], [], []
+    for t in tallies:
+        L = t.ledger.cpu().numpy()
+        rr = t.rr.cpu().numpy().astype(np.float64)
+        if rr.shape[1] != nr:
+            raise ValueError("the timed run's R(r) bins differ from the fixture's")
+        Rd.append(L[A.PMO_L_RD] / photons)
+        Tt.append(L[A.PMO_L_TT] / photons)
+        Rr.append((rr[A.PMO_RR_TOP] + rr[A.PMO_RR_LAT_NEG]) / (area * photons))
+        Tr.append((rr[A.PMO_RR_BOTTOM] + rr[A.PMO_RR_LAT_POS]) / (area * photons))
+
+    def mse(x):
+        x = np.asarray(x, np.float64)
+        se = x.std(axis=0, ddof=1) / np.sqrt(len(x)) if len(x) > 1 else np.zeros_like(x[0])
+        return x.mean(axis=0), se
+
+    out = {"fixture": "tests/golden/ref_c2_gaussian.json",
+           "reference_photons": int(g["nPh"]) * len(g["seeds"]),
+           "reference_code": "pymopt.voxel VoxelPlateModel(w_beam=1.0) (Numba), unmodified"}
+    zmax = 0.0
+    for key, mine in (("Rd", Rd), ("Tt", Tt)):
+        m, s_ = mse(mine)
+        rm, rs = mse(g[key])
+        z = float((m - rm) / np.hypot(s_, rs))
+        out[key] = {"ours": float(m), "reference": float(rm), "reference_se": float(rs),
+                    "z": z}
+        zmax = max(zmax, abs(z))
+    for key, mine in (("Rr", Rr), ("Tr", Tr)):
+        m, s_ = mse(mine)
+        ref = np.asarray(g[key], np.float64)
+        rm, rs = mse(ref)
+        keep = (np.count_nonzero(ref, axis=0) >= 5) & (rs > 0)
+        z = (m[keep] - rm[keep]) / np.hypot(s_[keep], rs[keep])
+        chi2 = float(np.sum(z ** 2))
+        out[key] = {"bins": int(keep.sum()), "chi2": chi2,
+                    "p": float(st.chi2.sf(chi2, int(keep.sum()))) if keep.any() else None,
+                    "zmax": float(np.max(np.abs(z))) if keep.any() else 0.0}
+        zmax = max(zmax, out[key]["zmax"])
+    out["zmax"] = zmax
+    out["within_3sigma"] = bool(abs(out["Rd"]["z"]) < 3 and abs(out["Tt"]["z"]) < 3 and
+                                all(out[k]["p"] is None or out[k]["p"] > 1e-3
+                                    for k in ("Rr", "Tr")))
     return out
 
 
@@ -442,6 +600,30 @@ def read_traffic():
         return None
     with open(path) as f:
         return json.load(f)
+
+
+def summary_dict(value, e2e, parity, batched, gradient, reference_gpu, cpu, roofline) -> dict:
+    """The headline figures of the run, one level deep."""
+    def get(d, *keys):
+        for k in keys:
+            if not isinstance(d, dict) or d.get(k) is None:
+                return None
+            d = d[k]
+        return d
+    return {
+        "photons_per_s": value,
+        "e2e_photons_per_s": get(e2e, "value"),
+        "fp32_issue_frac": get(roofline, "frac"),
+        "parity_zmax_vs_reference": get(parity, "zmax"),
+        "parity_within_3sigma": get(parity, "within_3sigma"),
+        "reference_cpu_photons_per_s": get(cpu, "value"),
+        "reference_cpu_single_process_photons_per_s": get(cpu, "single_process_value"),
+        "reference_cuvmc_on_b200_kernel_speedup": get(reference_gpu, "speedup_kernel"),
+        "batched_evals_per_s": get(batched, "batched_evals_per_s"),
+        "batched_ratio_vs_plain_reused": get(batched, "ratio"),
+        "batched_ratio_vs_single_launches": get(batched, "ratio_vs_single_launches"),
+        "gradient_c4_evals_per_s": get(gradient, "evals_per_s"),
+    }
 
 
 def main() -> int:
@@ -572,41 +754,54 @@ def main() -> int:
                "A": ledger[A.PMO_L_ABS] / nsteps_ph,
                "energy_balance_rel": (inflow - outflow) / inflow,
                "interactions_per_photon": counters[A.PMO_C_INTERACT] / nsteps_ph,
-               "crossings_per_photon": counters[A.PMO_C_CROSS] / nsteps_ph}
+               "crossings_per_photon": counters[A.PMO_C_CROSS] / nsteps_ph,
+               "extra_philox_draws_per_photon": counters[A.PMO_C_XDRAWS] / nsteps_ph}
+    parity = parity_vs_reference(tallies, photons) if rank == 0 else None
 
     # ---- e2e: engine API with host buffers --------------------------------
     e2e = None
     if not args.no_e2e:
-        pinned_labels = torch.from_numpy(prob.labels).pin_memory()
-        pinned_tabs = [torch.from_numpy(a).pin_memory() for a in (prob.ma, prob.ms, prob.g, prob.n)]
-        host_ledger = torch.empty(A.PMO_LEDGER_N, dtype=torch.float64).pin_memory()
-        host_rr = torch.empty(A.PMO_RR_CATS, 100, dtype=torch.float32).pin_memory()
-        host_cnt = torch.empty(A.PMO_COUNTERS_N, dtype=torch.int64).pin_memory()
-        h2d = pinned_labels.numel() + sum(t.numel() * 4 for t in pinned_tabs)
-        d2h = host_ledger.numel() * 8 + host_rr.numel() * 4 + host_cnt.numel() * 8
-        et = E.Tallies(dp, spec, photons)
+        # the plugin call a pymopt user makes, every step: build the model's
+        # volume on the host, start() (uploads the labels and optical tables,
+        # rebuilds the uniform-box map on the device, runs the transport,
+        # reads back the ledger and counters) and read Rd/Tt and R(r)
+        from pymonteopt_b200 import VoxelPlateModel
+        model = VoxelPlateModel(nPh=photons, w_beam=V.C2_W_BEAM, keep_exits=False,
+                                verbose=False, nr=100, dr=0.1, device=dev,
+                                threadnum=args.block_threads or None)
+        model.build(**V.C2_PARAMS)
+        model.start(4999 + 7919 * rank)            # warm-up of the model path
         e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                 for _ in range(args.steps)]
+        e_wall = []
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
         for k in range(args.steps):
             flush.zero_()
+            torch.cuda.synchronize()
+            w0_ = time.perf_counter()
             e_ev[k][0].record(stream)
-            dp.labels.copy_(pinned_labels, non_blocking=True)
-            for dst, src in zip((dp.ma, dp.ms, dp.g, dp.n), pinned_tabs):
-                dst.copy_(src, non_blocking=True)
-            et.zero_()
-            E.run_plain(dp, photons, seed=5000 + k, tallies=et, begin=begin0 + k * photons,
-                        block_threads=args.block_threads, blocks_per_sm=args.blocks_per_sm)
-            host_ledger.copy_(et.ledger, non_blocking=True)
-            host_rr.copy_(et.rr, non_blocking=True)
-            host_cnt.copy_(et.counters, non_blocking=True)
+            model.build(**V.C2_PARAMS)
+            model.start(5000 + k + 7919 * rank)
+            vals = model.getRdTtValues()
+            _, rr_host = model.get_Rr()
             e_ev[k][1].record(stream)
-        torch.cuda.synchronize()
+            torch.cuda.synchronize()
+            e_wall.append(time.perf_counter() - w0_)
         e_s = replicas.max_over_ranks(sum(a.elapsed_time(b) for a, b in e_ev) / 1e3, dev)
+        tal = model._tallies
+        h2d = model.model.voxel_model.nbytes + sum(
+            np.asarray(a, np.float32).nbytes for a in (model.model.ma, model.model.ms,
+                                                       model.model.g, model.model.n))
+        # start(): counters (check), ledger and counters (results); get_Rr: R(r)
+        d2h = 2 * tal.counters.numel() * 8 + tal.ledger.numel() * 8 + tal.rr.numel() * 4
         e2e = {"value": total_photons / e_s, "unit": UNIT,
-               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "path": "VoxelPlateModel(nPh, w_beam=1.0).build(**C2); start(seed); "
+                       "getRdTtValues(); get_Rr() -- every step",
+               "wall_s_per_step": float(np.mean(e_wall)), "Rd_last_step": vals["Rd"]}
+        del model
 
     batched = None
     if rank == 0 and world == 1 and not args.no_batched:
@@ -627,19 +822,32 @@ def main() -> int:
     if rank == 0 and world == 1 and not args.no_precision:
         precision = precision_leg(torch, dev)
 
-    cpu = None
+    cpu = cpu_port = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        r = cpu_oracle_rate(12.0)
-        cpu = {"value": r["value"], "unit": UNIT, "cores": r["threads"], "kind": "port",
-               "sample": f"{r['photons']} photons of the workload in {r['seconds']:.1f} s "
-                         f"(oracle/vmc_oracle.c FP32, OpenMP, {r['threads']} threads)"}
+        try:
+            cpu = reference_cpu_baseline(8.0)
+        except (RuntimeError, ImportError) as e:
+            cpu = {"value": None, "unit": UNIT, "cores": host_threads(), "kind": "reference",
+                   "sample": None, "unavailable": str(e)}
+        r = cpu_oracle_rate(4.0)
+        cpu_port = {"value": r["value"], "unit": UNIT, "cores": r["threads"], "kind": "port",
+                    "sample": f"{r['photons']} photons of the workload in {r['seconds']:.1f} s "
+                              f"(oracle/vmc_oracle.c FP32, OpenMP, {r['threads']} threads)"}
 
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     if rank != 0:
         return 0
+    # the long detail blocks come first and the compact summary last, so a
+    # record that keeps only the end of the line keeps the headline figures
     line = {
+        "fp32_vs_fp64": precision,
+        "reference_gpu": reference_gpu,
+        "gradient": gradient,
+        "batched": batched,
+        "cpu_port": cpu_port,
+        "results": results,
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * dev_s_max / args.steps,
@@ -650,13 +858,11 @@ def main() -> int:
         "cpu_baseline": cpu,
         "e2e": e2e,
         "gpu_launches": args.steps,
-        "batched": batched,
-        "reference_gpu": reference_gpu,
-        "gradient": gradient,
-        "fp32_vs_fp64": precision,
         "clocks": clk,
         "wall_s_timed_region": wall,
-        "results": results,
+        "parity": parity,
+        "summary": summary_dict(value, e2e, parity, batched, gradient, reference_gpu, cpu,
+                                roofline),
     }
     print(json.dumps(line), flush=True)
     return 0

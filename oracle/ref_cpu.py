@@ -190,6 +190,76 @@ def run_plate_seeds(params: dict, nph: int, seeds, model_kwargs: dict | None = N
         return pool.map(_plate_worker, jobs)
 
 
+_POOL_CASE = None
+
+
+def _pool_init(params, model_kwargs, path):
+    """Per worker process: import the reference and compile its kernel once."""
+    global _POOL_CASE
+    _POOL_CASE = (params, model_kwargs, path)
+    # Numba JIT warm-up (vmc_kernel takes idx % (nPh // 10), so nPh >= 10)
+    run_plate(params, 20, 7919, model_kwargs, nr=0, path=path)
+
+
+def _pool_task(args):
+    nph, seed = args
+    params, model_kwargs, path = _POOL_CASE
+    for attempt in range(8):
+        try:
+            r = run_plate(params, nph, seed + 100003 * attempt, model_kwargs, nr=0, path=path)
+            return r["seconds"], r["Rd"], attempt
+        except ZeroDivisionError:
+            continue   # the reference kernel's NaN direction (see _plate_worker)
+    raise RuntimeError("the reference kernel raised on 8 seeds in a row")
+
+
+class RefPool:
+    """``processes`` spawned workers running the reference's
+    ``VoxelPlateModel.build(**params).start()``; each has compiled the Numba
+    kernel before the first timed step."""
+
+    def __init__(self, params: dict, processes: int, model_kwargs: dict | None = None,
+                 path: str | None = None):
+        import multiprocessing as mp
+        self.processes = int(processes)
+        self.pool = mp.get_context("spawn").Pool(
+            self.processes, initializer=_pool_init, initargs=(params, model_kwargs, path))
+
+    def step(self, nph_per_process: int, seed: int) -> dict:
+        """Every process runs ``nph_per_process`` photons (distinct seeds) and
+        times its own start(); the step's rate is all photons over the slowest
+        process's seconds."""
+        jobs = [(int(nph_per_process), seed + 7919 * i) for i in range(self.processes)]
+        res = self.pool.map(_pool_task, jobs, chunksize=1)
+        secs = [r[0] for r in res]
+        return {"photons": self.processes * int(nph_per_process), "seconds": max(secs),
+                "seconds_min": min(secs), "value": self.processes * nph_per_process / max(secs),
+                "Rd_mean": float(np.mean([r[1] for r in res])),
+                "rerun_seeds": int(sum(r[2] for r in res))}
+
+    def close(self) -> None:
+        self.pool.close()
+        self.pool.join()
+
+
+def host_cpu() -> dict:
+    """CPU model and logical CPU count of this host (from /proc/cpuinfo)."""
+    model = "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    try:
+        n = len(os.sched_getaffinity(0))
+    except AttributeError:
+        n = os.cpu_count() or 1
+    return {"model": model, "logical_cpus": n}
+
+
 def _timed_worker(args):
     params, model_kwargs, nph, seed, path = args
     # Numba JIT warm-up (vmc_kernel takes idx % (nPh // 10), so nPh >= 10)
