@@ -90,6 +90,56 @@ def test_batched_statistics_match_oracle(cuda):
             assert abs(gm[q, i] - om[q]) <= 3 * se + 1e-6, (i, q, gm[q, i], om[q], se)
 
 
+def test_batched_rr_matches_oracle(cuda):
+    """R(r) of four C5-style slabs, 6 batched seeds against 6 oracle seeds on
+    the voxel plate of each slab: chi-square over the populated bins."""
+    from scipy import stats
+    from helpers import annulus_area, mean_se, profile_agreement
+    rng = np.random.default_rng(11)
+    params = []
+    for _ in range(4):
+        g = rng.uniform(0.7, 0.95)
+        params.append((float(np.exp(rng.uniform(np.log(0.005), np.log(0.5)))),
+                       float(np.exp(rng.uniform(np.log(0.5), np.log(5.0))) / (1 - g)), g,
+                       float(rng.uniform(1.33, 1.45)), float(rng.uniform(1.0, 8.0))))
+    nr, dr, N, No = 20, 0.2, 100000, 40000
+    mine = []
+    for seed in range(6):
+        sb = _batch(params, [N] * len(params), seed=700 + seed, nr=nr, dr=dr)
+        mine.append(sb.run(use_graph=False)["Rr"])
+    mine = np.array(mine)                      # (seeds, problems, nr)
+    area = annulus_area(nr, dr)
+    for i, (ma, ms, g, n, t) in enumerate(params):
+        prob = _voxel_slab(ma, ms, g, n, t)
+        ref = []
+        for seed in range(6):
+            o = oracle.run(prob, No, 1900 + seed, precision=A.PMO_FP32, nr=nr, dr=dr)
+            rr = o["rr"]
+            ref.append((rr[A.PMO_RR_TOP] + rr[A.PMO_RR_LAT_NEG]) / (area * No))
+        m, s_ = mean_se(mine[:, i])
+        z, chi2, dof = profile_agreement(m, s_, ref)
+        assert dof >= 10, (i, dof)
+        assert stats.chi2.sf(chi2, dof) > 1e-3, (i, chi2, dof, np.round(z, 2))
+        assert np.max(np.abs(z)) < 4.5, (i, np.round(z, 2))
+
+
+def test_plain_slab_evaluator_matches_batched_problem0(cuda):
+    """The reused-buffer comparator of the batched benchmark gives the same
+    Rd and per-label derivatives as the batched form's problem 0 (which draws
+    the plain kernel's Philox streams), within statistical error."""
+    ma, ms, g, n, t = 0.05, 8.0, 0.85, 1.4, 3.0
+    N = 400000
+    ev = B.PlainSlabEvaluator(N, nr=32, dr=0.1, device=cuda)
+    got = ev.evaluate(ma, ms, g, n, t, N, 123)
+    sb = _batch([(ma, ms, g, n, t)], [N], seed=123, nr=32, dr=0.1)
+    r = sb.run(use_graph=False)
+    assert abs(got["Rd"] - r["Rd"][0]) < 1e-3, (got["Rd"], r["Rd"][0])
+    # the evaluator's derivatives are of the sum of the R(r) bins
+    for key, col in (("dR_dma", "dRr_dma"), ("dR_dms", "dRr_dms")):
+        ref = float(r[col][0].sum())
+        assert abs(got[key] - ref) <= 0.05 * abs(ref) + 1e-6, (key, got[key], ref)
+
+
 def test_batched_gradients_match_pathwise_fd(cuda):
     base = (0.05, 6.0, 0.8, 1.37, 3.0)
     h = 3e-2
