@@ -95,8 +95,8 @@ static int PFX(trace)(const pmo_problem *P, const PFX(props_t) *tab,
             REAL rad = (REAL)P->beam_sigma * SQRT(-2 * LOG(u0));
             REAL xy[2] = {rad * COS(TWO_PI * u1), rad * SIN(TWO_PI * u1)};
             for (int a = 0; a < 2; ++a) {
-                REAL f = FLOOR(xy[a] / l);
-                REAL off = xy[a] - (f + (REAL)0.5) * l;
+                REAL f = FLOOR(xy[a] / l + (REAL)0.5);   /* nearest voxel centre */
+                REAL off = xy[a] - f * l;
                 if (FABS(off) >= hl) off = PFX(sgn)(off) * hl;
                 c[a] += (int)f;
                 p[a] = off;

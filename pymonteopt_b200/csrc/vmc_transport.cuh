@@ -550,7 +550,10 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
                 const uint4 rs = philox4x32_10(make_uint4(0u, 2u, (uint32_t)pid, (uint32_t)(pid >> 32)), kp.rk);
                 if (kp.source == PMO_SRC_GAUSSIAN) {
                     // x, y ~ N(0, sigma) (gaussianBeam, :267-287) by Box-Muller,
-                    // split into voxel index + offset in [-l/2, l/2] (:242-252)
+                    // split into the voxel whose centre is nearest and the
+                    // offset from that centre, in [-l/2, l/2]: the position
+                    // l * (index - centre) + offset is x exactly, as the
+                    // reference's split (:242-252) gives it
                     const R u0 = u01<R>(rs.x), u1 = u01<R>(rs.y);
                     const R rad = xmul((R)kp.beam_sigma, psqrt(xmul(R(2), pneglog(u0))));
                     R sn, cs;
@@ -558,8 +561,8 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
                     const R xy[2] = {xmul(rad, cs), xmul(rad, sn)};
 #pragma unroll
                     for (int a = 0; a < 2; ++a) {
-                        const R fl = floor(xdiv(xy[a], l));
-                        R off = xfma(-xadd(fl, R(0.5)), l, xy[a]);
+                        const R fl = floor(xadd(xdiv(xy[a], l), R(0.5)));
+                        R off = xfma(-fl, l, xy[a]);
                         if (fabs(off) >= hl) off = copysign(hl, off);
                         if (a == 0) { ix += (int)fl; px = off; }
                         else { iy += (int)fl; py = off; }
