@@ -316,45 +316,37 @@ __global__ void __launch_bounds__(512) vmc_batched_kernel(const BParams bp) {
         return true;
     };
 
-    // warp-uniform feed over the work items; `more` is the same on every lane
-    // (false once the queue is empty), so a pass costs one ballot unless a
-    // lane needs a new photon
+    // warp-uniform feed over the work items
     int item_p = -1;
     uint32_t i_next = 0, i_end = 0;
     bool active = false, more = true;
     for (;;) {
-        unsigned act = __ballot_sync(FULL, active);
-        if (more && act != FULL) {
-            unsigned need = ~act;
-            while (need) {
-                if (i_next >= i_end) {
-                    unsigned long long it = 0;
-                    if (lane == 0) it = atomicAdd(bp.work, 1ull);
-                    it = __shfl_sync(FULL, it, 0);
-                    if (it >= (unsigned long long)bp.n_items) {
-                        more = false;
-                        i_next = i_end = 0;
-                        break;
-                    }
-                    const pmo_batch_item itm = bp.items[it];
-                    item_p = (int)itm.problem;
-                    i_next = itm.begin;
-                    i_end = itm.begin + itm.count;
+        unsigned need = __ballot_sync(FULL, (!active) && more);
+        while (need) {
+            if (i_next >= i_end) {
+                unsigned long long it = 0;
+                if (lane == 0) it = atomicAdd(bp.work, 1ull);
+                it = __shfl_sync(FULL, it, 0);
+                if (it >= (unsigned long long)bp.n_items) {
+                    if ((need >> lane) & 1u) more = false;
+                    i_next = i_end = 0;
+                    need = 0;
+                    break;
                 }
-                const uint32_t avail = i_end - i_next;
-                const unsigned rank = __popc(need & ((1u << lane) - 1u));
-                const bool mine = ((need >> lane) & 1u) && rank < avail;
-                const unsigned taken = __ballot_sync(FULL, mine);
-                if (mine) active = start(item_p, i_next + rank);
-                i_next += __popc(taken);
-                need &= ~taken;
+                const pmo_batch_item itm = bp.items[it];
+                item_p = (int)itm.problem;
+                i_next = itm.begin;
+                i_end = itm.begin + itm.count;
             }
-            act = __ballot_sync(FULL, active);
+            const uint32_t avail = i_end - i_next;
+            const unsigned rank = __popc(need & ((1u << lane) - 1u));
+            const bool mine = ((need >> lane) & 1u) && rank < avail;
+            const unsigned taken = __ballot_sync(FULL, mine);
+            if (mine) active = start(item_p, i_next + rank);
+            i_next += __popc(taken);
+            need &= ~taken;
         }
-        if (!act) {
-            if (!more) break;
-            continue;
-        }
+        if (!__any_sync(FULL, active || more)) break;
         if (active) active = cycle();
     }
     flush();

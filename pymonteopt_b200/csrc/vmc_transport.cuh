@@ -886,42 +886,34 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
     };
 
     // ---- persistent photon loop: warp-uniform chunked feed ----
-    // `more` is the same on every lane: it turns false when the warp finds the
-    // photon pool empty.  A pass costs one ballot unless a lane needs a new
-    // photon (one lane in about fifteen passes per warp on C2).
     unsigned long long f_next = 0, f_end = 0;
     bool active = false, more = true;
     for (;;) {
-        unsigned act = __ballot_sync(FULL, active);
-        if (more && act != FULL) {
-            unsigned need = ~act;
-            while (need) {
-                if (f_next >= f_end) {
-                    unsigned long long b = 0;
-                    if (lane == 0) b = atomicAdd(kp.work, (unsigned long long)kChunk);
-                    b = __shfl_sync(FULL, b, 0);
-                    if (b >= N) {
-                        more = false;
-                        f_next = f_end = N;
-                        break;
-                    }
-                    f_next = b;
-                    f_end = b + kChunk < N ? b + kChunk : N;
+        unsigned need = __ballot_sync(FULL, (!active) && more);
+        while (need) {
+            if (f_next >= f_end) {
+                unsigned long long b = 0;
+                if (lane == 0) b = atomicAdd(kp.work, (unsigned long long)kChunk);
+                b = __shfl_sync(FULL, b, 0);
+                if (b >= N) {
+                    if ((need >> lane) & 1u) more = false;
+                    f_next = f_end = N;
+                    need = 0;
+                    break;
                 }
-                const unsigned long long avail = f_end - f_next;
-                const unsigned rank = __popc(need & ((1u << lane) - 1u));
-                const bool mine = ((need >> lane) & 1u) && (unsigned long long)rank < avail;
-                const unsigned taken = __ballot_sync(FULL, mine);
-                if (mine) active = start(f_next + rank);
-                f_next += __popc(taken);
-                need &= ~taken;
+                f_next = b;
+                f_end = b + kChunk < N ? b + kChunk : N;
             }
-            act = __ballot_sync(FULL, active);
+            const unsigned long long avail = f_end - f_next;
+            const unsigned rank = __popc(need & ((1u << lane) - 1u));
+            const bool mine = ((need >> lane) & 1u) && (unsigned long long)rank < avail;
+            const unsigned taken = __ballot_sync(FULL, mine);
+            if (mine) active = start(f_next + rank);
+            f_next += __popc(taken);
+            need &= ~taken;
         }
-        if (!act) {
-            if (!more) break;
-            continue;   // every new photon ended at its start; fetch more
-        }
+        if (!__any_sync(FULL, active || more)) break;
+        const unsigned act = __ballot_sync(FULL, active);
         if (active) active = cycle(act);
     }
 
