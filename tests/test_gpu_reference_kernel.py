@@ -6,7 +6,8 @@
 reference's launch and read-back (``oracle/ref_gpu.py``).  Its RNG (cuRAND
 XORWOW seeded per thread) differs from this kernel's Philox streams, so the
 comparison is statistical: Rd and Tt within 3 sigma of the seed-to-seed
-standard error, and R(r)/T(r) by a chi-square test over the populated bins.
+standard error (40 seeds a side), and R(r)/T(r) by a chi-square test over
+the populated bins.
 """
 import os
 import sys
@@ -70,8 +71,10 @@ CASES = {
 def test_statistics_match_reference_gpu_kernel(cuda, case):
     make, n_per, nr, dr = CASES[case]
     prob = make()
-    mine = _ours(prob, range(300, 310), n_per, nr, dr, cuda)
-    ref = _theirs(prob, range(1, 11), n_per, nr, dr, cuda)
+    # 40 seeds a side: with few seeds the per-bin z-scores follow a t
+    # distribution and the chi-square over 100 bins is exceeded too easily
+    mine = _ours(prob, range(300, 340), n_per, nr, dr, cuda)
+    ref = _theirs(prob, range(1, 41), n_per, nr, dr, cuda)
     for q in ("Rd", "Tt"):
         m, s = mean_se(mine[q])
         rm, rs = mean_se(ref[q])

@@ -61,10 +61,10 @@ def _fresnel_unpolarised(ai, n1, n2):
 @pytest.mark.parametrize("case,n_per,precision", [
     ("c1", 20000, A.PMO_FP32), ("c1", 20000, A.PMO_FP64),
     ("thin_slab", 20000, A.PMO_FP32), ("semi_inf_mismatch", 20000, A.PMO_FP32),
-    ("three_layer", 20000, A.PMO_FP32), ("c2_pencil", 20000, A.PMO_FP32),
-    ("c2_gaussian", 50000, A.PMO_FP32), ("c3", 20000, A.PMO_FP32),
-    ("oblique", 20000, A.PMO_FP32), ("oblique_specular", 20000, A.PMO_FP32),
-    ("ex_first_layer", 20000, A.PMO_FP32)])
+    ("three_layer", 20000, A.PMO_FP32), ("c2_pencil", 10000, A.PMO_FP32),
+    ("c2_gaussian", 40000, A.PMO_FP32), ("c3", 10000, A.PMO_FP32),
+    ("oblique", 10000, A.PMO_FP32), ("oblique_specular", 10000, A.PMO_FP32),
+    ("ex_first_layer", 10000, A.PMO_FP32)])
 def test_oracle_matches_reference_fixtures(case, n_per, precision):
     # the oblique beam with initial_refrect_by_angle has no reference run of
     # its own (the reference indexes past its state arrays with it); its
@@ -77,7 +77,8 @@ def test_oracle_matches_reference_fixtures(case, n_per, precision):
         p = g["params"]
         rd_shift = float(_fresnel_unpolarised(g["model_kwargs"]["beam_angle"], p["n_air"],
                                               p["n"][0]))
-    Rd, Tt, Rr, Tr = _seed_batches(prob, range(200, 210), n_per, g["nr"], g["dr"], precision)
+    # 20 oracle seeds: the z-scores use the seed-to-seed spread of both sides
+    Rd, Tt, Rr, Tr = _seed_batches(prob, range(200, 220), n_per, g["nr"], g["dr"], precision)
     for mine, ref, shift in ((Rd, g["Rd"], rd_shift), (Tt, g["Tt"], 0.0)):
         m, s = mean_se(mine)
         rm, rs = mean_se(ref)
