@@ -375,6 +375,96 @@ int pmo_run_batched(const pmo_batch *batch, const pmo_launch *launch, void *work
    [1/mm^2]) from the sums of pmo_run_batched. */
 int pmo_batch_finalize(const pmo_batch *batch, double *results, double *rr, void *stream);
 
+/* ---- batched layered slabs ------------------------------------------- */
+
+/* One layer of a laterally infinite layered slab: a PlateModel stack
+   (pymopt/voxel_gpu/_classes.py:396-459) with x_size, y_size unbounded. */
+typedef struct pmo_layer {
+    float ma, ms, g, n;           /* mu_a, mu_s [1/mm], anisotropy, index */
+    float thickness;              /* [mm] */
+} pmo_layer;
+
+#define PMO_MAX_LAYERS 8
+
+/* One problem: layers [first_layer, first_layer + n_layers) of the layer
+   table, top to bottom.  Photons enter at the origin of the top face along +z
+   with weight 1 - Rsp, Rsp = ((n_ambient - n_top) / (n_ambient + n_top))^2
+   (pymopt/voxel_gpu/_classes.py:204-221). */
+typedef struct pmo_stack {
+    uint32_t first_layer;
+    uint32_t n_layers;            /* 1 .. PMO_MAX_LAYERS */
+    float n_ambient;
+    float dr;                     /* R(r) bin width [mm] */
+    uint32_t photons;             /* photon budget */
+} pmo_stack;
+
+/* Per-problem raw sums (double) of pmo_run_stack_batch: the scalars below,
+   then for layer i at PMO_SS_LAYER0 + 4 i: sum w L_i and sum w n_i of top
+   exits (+0, +1) and of bottom exits (+2, +3), with L_i the photon's path
+   length and n_i its interactions in layer i. */
+#define PMO_SS_RD      0
+#define PMO_SS_TT      1
+#define PMO_SS_ABS     2
+#define PMO_SS_WINIT   3
+#define PMO_SS_RGAIN   4
+#define PMO_SS_RLOSS   5
+#define PMO_SS_ERRW    6
+#define PMO_SS_INTER   7
+#define PMO_SS_LAYER0  8
+#define PMO_SS_N       40         /* PMO_SS_LAYER0 + 4 * PMO_MAX_LAYERS */
+
+/* Per-problem results of pmo_stack_batch_finalize (double): Rd, Tt, A, the
+   energy residual, then for layer i at PMO_SR_LAYER0 + 4 i: dRd/dmu_a_i,
+   dRd/dmu_s_i, dTt/dmu_a_i, dTt/dmu_s_i (perturbation Monte Carlo:
+   d/dmu_a_i = -E[w L_i], d/dmu_s_i = E[w (n_i / mu_s_i - L_i)]). */
+#define PMO_SR_RD      0
+#define PMO_SR_TT      1
+#define PMO_SR_A       2
+#define PMO_SR_BALANCE 3
+#define PMO_SR_LAYER0  4
+#define PMO_SR_N       36         /* PMO_SR_LAYER0 + 4 * PMO_MAX_LAYERS */
+
+/* R(r) bin record of a stack problem: PMO_SB_N floats per bin: sum w of the
+   top exits in (i dr, (i+1) dr], then per layer sum w L_i and sum w n_i.
+   Finalised R(r) has the same layout in doubles: R, then per layer
+   dR/dmu_a_i and dR/dmu_s_i [1/mm^2]. */
+#define PMO_SB_N       17         /* 1 + 2 * PMO_MAX_LAYERS */
+
+typedef struct pmo_stack_batch {
+    const pmo_stack *stacks;      /* device array of n_problems */
+    int32_t n_problems;
+    const pmo_layer *layers;      /* device layer table */
+    int32_t n_layer_rows;
+    const pmo_batch_item *items;  /* device work queue of n_items, in order */
+    int32_t n_items;
+    uint64_t seed;
+    int32_t nr;                   /* R(r) bins per problem */
+    double *sums;                 /* n_problems * PMO_SS_N, accumulated */
+    float *bins;                  /* n_problems * nr * PMO_SB_N, accumulated */
+    uint32_t *remaining;          /* per problem photons in flight, or NULL */
+    unsigned long long *t_done;   /* per problem completion time, or NULL */
+    int32_t precision;            /* PMO_FP32 or PMO_FP64 */
+    uint32_t max_events;          /* 0 = 2^26 */
+} pmo_stack_batch;
+
+/*
+ * Many layered slab problems in one persistent launch, forward and gradient
+ * together: the batched form of pmo_run_batched for PlateModel stacks.  Same
+ * work queue, Philox layout (problem p uses stream word 4p + s) and transport
+ * rules; a stack of one layer follows the photons of pmo_run_batched.  At an
+ * inner interface with equal refractive indices the photon keeps its optical
+ * depth and takes the next layer's mu (:154-167); otherwise Fresnel /
+ * refraction as at an outer face.  Sums go to global memory with atomics.
+ * No counterpart in the reference, which runs one problem per launch.
+ */
+int pmo_run_stack_batch(const pmo_stack_batch *batch, const pmo_launch *launch,
+                        void *workspace, size_t workspace_bytes, void *stream);
+
+/* Per-problem results (n_problems * PMO_SR_N doubles) and R(r) with its
+   per-layer derivatives (n_problems * nr * PMO_SB_N doubles) from the sums. */
+int pmo_stack_batch_finalize(const pmo_stack_batch *batch, double *results, double *rr,
+                             void *stream);
+
 /*
  * pmo_run_plain without a caller-allocated workspace.  No counterpart in the
  * reference.  For callers that cannot allocate device memory themselves (a

@@ -202,6 +202,39 @@ class PmoBatch(C.Structure):
     ]
 
 
+PMO_MAX_LAYERS = 8
+PMO_SS_RD, PMO_SS_TT, PMO_SS_ABS, PMO_SS_WINIT = 0, 1, 2, 3
+PMO_SS_RGAIN, PMO_SS_RLOSS, PMO_SS_ERRW, PMO_SS_INTER = 4, 5, 6, 7
+PMO_SS_LAYER0 = 8
+PMO_SS_N = 40
+PMO_SR_RD, PMO_SR_TT, PMO_SR_A, PMO_SR_BALANCE = 0, 1, 2, 3
+PMO_SR_LAYER0 = 4
+PMO_SR_N = 36
+PMO_SB_N = 17
+
+
+class PmoLayer(C.Structure):
+    _fields_ = [("ma", C.c_float), ("ms", C.c_float), ("g", C.c_float), ("n", C.c_float),
+                ("thickness", C.c_float)]
+
+
+class PmoStack(C.Structure):
+    _fields_ = [("first_layer", C.c_uint32), ("n_layers", C.c_uint32),
+                ("n_ambient", C.c_float), ("dr", C.c_float), ("photons", C.c_uint32)]
+
+
+class PmoStackBatch(C.Structure):
+    _fields_ = [
+        ("stacks", C.c_void_p), ("n_problems", C.c_int32),
+        ("layers", C.c_void_p), ("n_layer_rows", C.c_int32),
+        ("items", C.c_void_p), ("n_items", C.c_int32),
+        ("seed", C.c_uint64), ("nr", C.c_int32),
+        ("sums", C.c_void_p), ("bins", C.c_void_p),
+        ("remaining", C.c_void_p), ("t_done", C.c_void_p),
+        ("precision", C.c_int32), ("max_events", C.c_uint32),
+    ]
+
+
 class PmoObdParams(C.Structure):
     _fields_ = [
         ("outer_d1", C.c_double), ("ct1", C.c_double), ("r1", C.c_double),

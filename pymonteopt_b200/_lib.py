@@ -33,6 +33,10 @@ SIGNATURES = {
                                   C.c_size_t, C.c_void_p]),
     "pmo_batch_finalize": (C.c_int, [C.POINTER(A.PmoBatch), C.c_void_p, C.c_void_p,
                                      C.c_void_p]),
+    "pmo_run_stack_batch": (C.c_int, [C.POINTER(A.PmoStackBatch), C.POINTER(A.PmoLaunch),
+                                      C.c_void_p, C.c_size_t, C.c_void_p]),
+    "pmo_stack_batch_finalize": (C.c_int, [C.POINTER(A.PmoStackBatch), C.c_void_p, C.c_void_p,
+                                           C.c_void_p]),
     "pmo_run_plain_static": (C.c_int, [C.POINTER(A.PmoProblem), C.POINTER(A.PmoTallies),
                                        C.POINTER(A.PmoLaunch), C.c_void_p]),
     "pmo_cuvmc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,

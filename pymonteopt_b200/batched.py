@@ -9,6 +9,11 @@ Monte Carlo derivatives with respect to mu_a and mu_s.  The launch sequence
 (clearing the sums, the kernel, the FP64 finalisation) is captured in a CUDA
 graph and replayed.
 
+:class:`StackBatch` does the same for layered slabs (PlateModel stacks of up to
+``PMO_MAX_LAYERS`` layers with unbounded lateral size) through
+``pmo_run_stack_batch``, with the derivatives of every output with respect to
+each layer's mu_a and mu_s.
+
 The launch shape (threads per block, photons per work item) and where the
 per-problem sums gather (privatised per thread in shared memory, or straight
 to global memory) are chosen by a small autotuner. It times candidates on a
@@ -261,6 +266,146 @@ class SlabBatch:
                                        for m, v in by_mode.items()}}
         _TUNE_CACHE[sig] = self.tune_table
         return best
+
+
+LAYER_DTYPE = np.dtype([("ma", "<f4"), ("ms", "<f4"), ("g", "<f4"), ("n", "<f4"),
+                        ("thickness", "<f4")])
+STACK_DTYPE = np.dtype([("first_layer", "<u4"), ("n_layers", "<u4"), ("n_ambient", "<f4"),
+                        ("dr", "<f4"), ("photons", "<u4")])
+
+
+class StackBatch:
+    """A batch of layered slab problems resident on one GPU: PlateModel stacks
+    (pymopt/voxel_gpu/_classes.py:396-459) with unbounded lateral size, run by
+    ``pmo_run_stack_batch`` in one persistent launch with forward and
+    per-layer gradient together.
+
+    ``stacks``: one sequence of layers per problem, top layer first, each
+    layer ``(ma, ms, g, n, thickness)`` [1/mm, 1/mm, -, -, mm], at most
+    ``PMO_MAX_LAYERS`` layers; ``photons``: budget per problem;
+    ``n_ambient``: scalar or per problem.  ``dr`` [mm] and ``nr`` set the R(r)
+    bins of every problem.  A stack of one layer follows the photons of
+    :class:`SlabBatch` on the same seed.
+    """
+
+    def __init__(self, stacks, photons, *, n_ambient=1.0, nr: int = 32, dr: float = 0.1,
+                 seed: int = 0, precision: int = A.PMO_FP32, device=None,
+                 block_threads: int = 128, chunk: int = 256):
+        load()
+        self.device = E.require_cuda(device)
+        P = len(stacks)
+        photons = np.broadcast_to(np.asarray(photons, np.int64), (P,))
+        n_amb = np.broadcast_to(np.asarray(n_ambient, np.float32), (P,))
+        rows = []
+        st = np.zeros(P, STACK_DTYPE)
+        for i, layers in enumerate(stacks):
+            layers = [tuple(float(v) for v in L) for L in layers]
+            if not 1 <= len(layers) <= A.PMO_MAX_LAYERS:
+                raise ValueError(f"problem {i}: 1 to {A.PMO_MAX_LAYERS} layers")
+            for ma, ms, g, n, t in layers:
+                if not (t > 0 and ma >= 0 and ms >= 0 and abs(g) <= 1 and n > 0):
+                    raise ValueError(f"problem {i}: thickness > 0, ma, ms >= 0, |g| <= 1, n > 0")
+            st[i] = (len(rows), len(layers), n_amb[i], dr, photons[i])
+            rows.extend(layers)
+        if np.any(photons < 1) or np.any(photons >= 2**32):
+            raise ValueError("photon budgets must lie in [1, 2^32)")
+        table = np.array(rows, LAYER_DTYPE)
+        self.host_stacks, self.host_layers = st, table
+        self.n_layers = st["n_layers"].astype(int)
+        self.P = P
+        self.nr = int(nr)
+        self.seed = int(seed)
+        self.precision = precision
+        self.block_threads = int(block_threads)
+        dev = self.device
+        self.stacks = torch.from_numpy(st.view(np.uint8).copy()).to(dev)
+        self.layers = torch.from_numpy(table.view(np.uint8).copy()).to(dev)
+        self.sums = torch.zeros(P, A.PMO_SS_N, dtype=torch.float64, device=dev)
+        self.bins = torch.zeros(P, max(self.nr, 1), A.PMO_SB_N, dtype=torch.float32, device=dev)
+        self.remaining = torch.zeros(P, dtype=torch.int32, device=dev)
+        self.budget = torch.from_numpy(photons.astype(np.int32)).to(dev)
+        self.t_done = torch.zeros(P, dtype=torch.int64, device=dev)
+        self.results = torch.zeros(P, A.PMO_SR_N, dtype=torch.float64, device=dev)
+        self.rr = torch.zeros(P, max(self.nr, 1), A.PMO_SB_N, dtype=torch.float64, device=dev)
+        self.workspace = torch.zeros(int(load().pmo_workspace_bytes()), dtype=torch.uint8,
+                                     device=dev)
+        self.chunk = int(chunk)
+        items = build_items(photons, self.chunk)
+        self.items = torch.from_numpy(items.view(np.uint8).copy()).to(dev)
+        self.n_items = len(items)
+        self.graph = None
+
+    def _struct(self) -> A.PmoStackBatch:
+        b = A.PmoStackBatch()
+        b.stacks, b.n_problems = self.stacks.data_ptr(), self.P
+        b.layers, b.n_layer_rows = self.layers.data_ptr(), len(self.host_layers)
+        b.items, b.n_items = self.items.data_ptr(), self.n_items
+        b.seed = self.seed & 0xFFFFFFFFFFFFFFFF
+        b.nr = self.nr
+        b.sums, b.bins = self.sums.data_ptr(), self.bins.data_ptr()
+        b.remaining, b.t_done = self.remaining.data_ptr(), self.t_done.data_ptr()
+        b.precision = self.precision
+        return b
+
+    def launch(self, stream=None) -> None:
+        """Enqueue one evaluation: clear sums, run the batch, finalise."""
+        self.sums.zero_()
+        self.bins.zero_()
+        self.remaining.copy_(self.budget)
+        self.t_done.zero_()
+        b = self._struct()
+        lib = load()
+        check(lib.pmo_run_stack_batch(C.byref(b), C.byref(A.PmoLaunch(self.block_threads, 0)),
+                                      C.c_void_p(self.workspace.data_ptr()),
+                                      self.workspace.numel(), E._stream_handle(stream)),
+              "pmo_run_stack_batch")
+        check(lib.pmo_stack_batch_finalize(
+            C.byref(b), C.c_void_p(self.results.data_ptr()),
+            C.c_void_p(self.rr.data_ptr()) if self.nr > 0 else None, E._stream_handle(stream)),
+            "pmo_stack_batch_finalize")
+
+    def capture(self) -> "torch.cuda.CUDAGraph":
+        """Capture :meth:`launch` in a CUDA graph (warms up once first)."""
+        s = torch.cuda.Stream(device=self.device)
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            self.launch()
+        torch.cuda.current_stream().wait_stream(s)
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.launch()
+        self.graph = g
+        return g
+
+    def run(self, use_graph: bool = True) -> dict:
+        """One evaluation; returns host results (synchronises)."""
+        if use_graph:
+            if self.graph is None:
+                self.capture()
+            self.graph.replay()
+        else:
+            self.launch()
+        return self.fetch()
+
+    def fetch(self) -> dict:
+        res = self.results.cpu().numpy()
+        rr = self.rr.cpu().numpy()
+        ws = self.workspace[8:16].cpu().numpy().view(np.uint64)[0]
+        td = self.t_done.cpu().numpy().view(np.uint64)
+        K = A.PMO_MAX_LAYERS
+        lay = res[:, A.PMO_SR_LAYER0:A.PMO_SR_LAYER0 + 4 * K].reshape(self.P, K, 4)
+        return {
+            "Rd": res[:, A.PMO_SR_RD], "Tt": res[:, A.PMO_SR_TT], "A": res[:, A.PMO_SR_A],
+            "balance": res[:, A.PMO_SR_BALANCE],
+            # per problem and layer (layers beyond a problem's own are 0)
+            "dRd_dma": lay[:, :, 0], "dRd_dms": lay[:, :, 1],
+            "dTt_dma": lay[:, :, 2], "dTt_dms": lay[:, :, 3],
+            "Rr": rr[:, :, 0], "dRr_dma": rr[:, :, 1::2][:, :, :K],
+            "dRr_dms": rr[:, :, 2::2][:, :, :K],
+            "completion_ms": (td.astype(np.float64) - float(ws)) / 1e6,
+            "sums": self.sums.cpu().numpy(), "n_layers": self.n_layers,
+        }
 
 
 def time_batch(batch: SlabBatch, reps: int = 3) -> dict:

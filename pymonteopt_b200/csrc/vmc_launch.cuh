@@ -5,6 +5,7 @@
 #include <atomic>
 
 #include "vmc_batched.cuh"
+#include "vmc_stack.cuh"
 #include "vmc_transport.cuh"
 
 namespace pmo {
@@ -115,6 +116,26 @@ cudaError_t launch_batched_r(const BParams &bp, int threads, int blocks_per_sm, 
     if (occ < 1) return cudaErrorInvalidConfiguration;
     const int per_sm = blocks_per_sm > 0 && blocks_per_sm < occ ? blocks_per_sm : occ;
     kern<<<sms * per_sm, threads, smem, s>>>(bp);
+    return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_stack_r(const SParams &sp, int threads, int blocks_per_sm, cudaStream_t s) {
+    auto kern = vmc_stack_kernel<R>;
+    const size_t smem = (size_t)threads * 2 * PMO_MAX_LAYERS * sizeof(R);
+    cudaError_t e;
+    if (smem > 48 * 1024) {
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    const int sms = device_sm_count();
+    if (sms <= 0) return cudaErrorNoDevice;
+    int occ = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, threads, smem);
+    if (e != cudaSuccess) return e;
+    if (occ < 1) return cudaErrorInvalidConfiguration;
+    const int per_sm = blocks_per_sm > 0 && blocks_per_sm < occ ? blocks_per_sm : occ;
+    kern<<<sms * per_sm, threads, smem, s>>>(sp);
     return cudaGetLastError();
 }
 

@@ -15,4 +15,7 @@ cudaError_t launch_grad_f32(const KParams &kp, int props, int threads, int bps,
 cudaError_t launch_batched_f32(const BParams &bp, int threads, int bps, cudaStream_t s) {
     return launch_batched_r<float>(bp, threads, bps, s);
 }
+cudaError_t launch_stack_f32(const SParams &sp, int threads, int bps, cudaStream_t s) {
+    return launch_stack_r<float>(sp, threads, bps, s);
+}
 }  // namespace pmo

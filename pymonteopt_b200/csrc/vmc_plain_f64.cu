@@ -16,4 +16,7 @@ cudaError_t launch_grad_f64(const KParams &kp, int props, int threads, int bps,
 cudaError_t launch_batched_f64(const BParams &bp, int threads, int bps, cudaStream_t s) {
     return launch_batched_r<double>(bp, threads, bps, s);
 }
+cudaError_t launch_stack_f64(const SParams &sp, int threads, int bps, cudaStream_t s) {
+    return launch_stack_r<double>(sp, threads, bps, s);
+}
 }  // namespace pmo

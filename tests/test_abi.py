@@ -114,6 +114,8 @@ def _c_offsets(struct_name, fields):
                                       (A.PmoLaunch, "pmo_launch"), (A.PmoGrad, "pmo_grad"),
                                       (A.PmoSlab, "pmo_slab"), (A.PmoBatchItem, "pmo_batch_item"),
                                       (A.PmoBatch, "pmo_batch"),
+                                      (A.PmoLayer, "pmo_layer"), (A.PmoStack, "pmo_stack"),
+                                      (A.PmoStackBatch, "pmo_stack_batch"),
                                       (A.PmoObdParams, "pmo_obd_params")])
 def test_struct_layout_matches_header(cls, name):
     fields = [f[0] for f in cls._fields_]
