@@ -55,6 +55,8 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched+gradient vs plain comparison (4096 slabs)")
+    ap.add_argument("--no-stacks", action="store_true",
+                    help="skip the layered batch vs plain comparison (1024 skin stacks)")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference's own cuVMC kernel on the 256^3 volume")
     ap.add_argument("--ref-gpu-photons", type=float, default=1e7)
@@ -602,7 +604,8 @@ def read_traffic():
         return json.load(f)
 
 
-def summary_dict(value, e2e, parity, batched, gradient, reference_gpu, cpu, roofline) -> dict:
+def summary_dict(value, e2e, parity, batched, gradient, reference_gpu, cpu, roofline,
+                 stacks=None) -> dict:
     """The headline figures of the run, one level deep."""
     def get(d, *keys):
         for k in keys:
@@ -623,6 +626,8 @@ def summary_dict(value, e2e, parity, batched, gradient, reference_gpu, cpu, roof
         "batched_ratio_vs_plain_reused": get(batched, "ratio"),
         "batched_ratio_vs_single_launches": get(batched, "ratio_vs_single_launches"),
         "gradient_c4_evals_per_s": get(gradient, "evals_per_s"),
+        "stacks_evals_per_s": get(stacks, "batched_evals_per_s"),
+        "stacks_ratio_vs_plain_reused": get(stacks, "ratio"),
     }
 
 
@@ -810,6 +815,12 @@ def main() -> int:
         from pymonteopt_b200 import batched as B
         batched = B.batched_vs_plain(count=4096, device=dev)
 
+    stacks = None
+    if rank == 0 and world == 1 and not args.no_stacks:
+        # layered problems: a sweep of three-layer skin stacks in one launch
+        from pymonteopt_b200 import batched as B
+        stacks = B.stacks_vs_plain(count=1024, device=dev)
+
     reference_gpu = None
     if rank == 0 and world == 1 and not args.no_reference_gpu:
         reference_gpu = reference_gpu_leg(torch, dev, int(args.ref_gpu_photons))
@@ -846,6 +857,7 @@ def main() -> int:
         "reference_gpu": reference_gpu,
         "gradient": gradient,
         "batched": batched,
+        "stacks": stacks,
         "cpu_port": cpu_port,
         "results": results,
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -862,7 +874,7 @@ def main() -> int:
         "wall_s_timed_region": wall,
         "parity": parity,
         "summary": summary_dict(value, e2e, parity, batched, gradient, reference_gpu, cpu,
-                                roofline),
+                                roofline, stacks),
     }
     print(json.dumps(line), flush=True)
     return 0

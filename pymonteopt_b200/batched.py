@@ -603,6 +603,112 @@ def batched_vs_plain(count: int = 4096, plain_sample: int = 48, seed: int = 0, n
     }
 
 
+class PlainStackEvaluator:
+    """Forward + per-layer gradient of one skin stack at a time through the
+    per-problem plain API with every buffer reused: the comparator of the
+    layered batch.  All problems of the sweep share the layer thicknesses, so
+    one resident voxel plate (20 x 20 mm, 0.05 mm voxels, its box map built
+    once) serves them all; per problem the three layers' mu_a and mu_s are
+    copied in, then the scored forward run and the per-label replay run and
+    Rd and its six derivatives are read back."""
+
+    def __init__(self, layers, max_photons: int, nr: int = 32, dr: float = 0.1, device=None,
+                 lateral_mm: float = 20.0, voxel_mm: float = 0.05):
+        from . import volumes as V
+        prob = V.plate_problem(dict(x_size=lateral_mm, y_size=lateral_mm, voxel_space=voxel_mm,
+                                    thickness=[L[4] for L in layers], n=[L[3] for L in layers],
+                                    n_air=1.0, ma=[L[0] for L in layers],
+                                    ms=[L[1] for L in layers], g=[L[2] for L in layers]))
+        self.nl = len(layers)
+        self.dp = E.DeviceProblem(prob, device)
+        dev = self.dp.device
+        self.nr, self.dr = int(nr), float(dr)
+        self.tal = E.Tallies(self.dp, E.TallySpec(nr=nr, dr=dr), 0)
+        self.score_bin = torch.empty(int(max_photons), dtype=torch.int32, device=dev)
+        self.score_w = torch.empty(int(max_photons), dtype=torch.float32, device=dev)
+        area = torch.tensor(annulus_area_mm2(nr, dr), dtype=torch.float64, device=dev)
+        self.coef = torch.zeros(A.PMO_RR_CATS, nr, dtype=torch.float32, device=dev)
+        self.coef[A.PMO_RR_TOP] = (1.0 / area).float()
+        self.coef[A.PMO_RR_LAT_NEG] = self.coef[A.PMO_RR_TOP]
+        self.grad_sums = torch.zeros(2, len(self.dp.host.n), dtype=torch.float64, device=dev)
+        self.gcnt = torch.zeros(A.PMO_G_COUNTERS_N, dtype=torch.int64, device=dev)
+        self.tabs = torch.zeros(2, len(self.dp.host.n), dtype=torch.float32)
+        self.max_photons = int(max_photons)
+
+    def evaluate(self, layers, photons: int, seed: int) -> dict:
+        photons = int(photons)
+        lib = load()
+        dp = self.dp
+        for i, L in enumerate(layers):
+            self.tabs[0, i], self.tabs[1, i] = float(L[0]), float(L[1])
+        dp.ma.copy_(self.tabs[0], non_blocking=True)
+        dp.ms.copy_(self.tabs[1], non_blocking=True)
+        self.tal.zero_()
+        self.grad_sums.zero_()
+        self.gcnt.zero_()
+        stream = E._stream_handle()
+        launch = A.PmoLaunch(0, 0)
+        ws = C.c_void_p(dp.workspace.data_ptr())
+        s = dp.struct(seed, 0, photons, A.PMO_FP32, A.PMO_FLAG_SCORE_RECORD)
+        ts = self.tal.struct()
+        ts.score_bin, ts.score_w = self.score_bin.data_ptr(), self.score_w.data_ptr()
+        check(lib.pmo_run_plain(C.byref(s), C.byref(ts), C.byref(launch), ws,
+                                dp.workspace.numel(), stream), "pmo_run_plain (scored)")
+        gr = A.PmoGrad()
+        gr.coef = self.coef.data_ptr()
+        gr.nr, gr.dr = self.nr, self.dr
+        gr.score_bin, gr.score_w = self.score_bin.data_ptr(), self.score_w.data_ptr()
+        gr.d_ma_label = self.grad_sums[0].data_ptr()
+        gr.d_ms_label = self.grad_sums[1].data_ptr()
+        gr.counters = self.gcnt.data_ptr()
+        s = dp.struct(seed, 0, photons, A.PMO_FP32)
+        check(lib.pmo_run_grad(C.byref(s), C.byref(gr), C.byref(launch), ws,
+                               dp.workspace.numel(), stream), "pmo_run_grad")
+        led = self.tal.ledger.cpu().numpy()          # synchronises
+        g = self.grad_sums[:, :self.nl].cpu().numpy() / photons
+        return {"Rd": led[A.PMO_L_RD] / photons, "dR_dma": g[0], "dR_dms": g[1]}
+
+
+def stacks_vs_plain(count: int = 1024, plain_sample: int = 48, seed: int = 0, nr: int = 32,
+                    dr: float = 0.1, device=None) -> dict:
+    """The layered batch on a skin sweep (volumes.skin_stack_sweep): ``count``
+    three-layer stacks, forward + per-layer gradient in one graph-captured
+    launch, against the per-problem plain path with reused buffers on a
+    random sample of the same problems."""
+    from . import volumes as V
+    sw = V.skin_stack_sweep(seed=seed, count=count)
+    stacks, photons = sw["stacks"], sw["n_photons"]
+    sb = StackBatch(stacks, photons, nr=nr, dr=dr, seed=seed + 1, device=device)
+    sb.capture()
+    tb = time_batch(sb, reps=3)
+    res = sb.fetch()
+    comp = res["completion_ms"]
+    rng = np.random.default_rng(seed + 11)
+    pick = rng.choice(count, size=min(plain_sample, count), replace=False)
+    ev = PlainStackEvaluator(V.SKIN_LAYERS, int(photons.max()), nr=nr, dr=dr, device=device)
+    for i in pick[:2]:
+        ev.evaluate(stacks[i], 1000, seed + 1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in pick:
+        ev.evaluate(stacks[i], int(photons[i]), seed + 1)
+    torch.cuda.synchronize()
+    plain_rate = len(pick) / (time.perf_counter() - t0)
+    total = float(photons.sum())
+    return {
+        "problems": count, "layers_per_problem": 3, "photons": total,
+        "batched_seconds": tb["seconds"], "batched_evals_per_s": tb["evals_per_s"],
+        "batched_photons_per_s": total / tb["seconds"],
+        "plain_evals_per_s": plain_rate,
+        "plain_path": "PlainStackEvaluator: one resident 20 x 20 mm plate at 0.05 mm, optics "
+                      "rewritten per problem, scored forward + per-label replay + read-back",
+        "plain_sample": len(pick), "ratio": tb["evals_per_s"] / plain_rate,
+        "p50_completion_ms": float(np.percentile(comp, 50)),
+        "p99_completion_ms": float(np.percentile(comp, 99)),
+        "max_energy_residual": float(np.max(np.abs(res["balance"]))),
+    }
+
+
 def main(argv=None) -> int:
     """``python -m pymonteopt_b200.batched``: time graph replays of the C5
     slab batch (forward + gradient) and print one JSON line."""

@@ -151,3 +151,24 @@ def c5_slab_batch(seed: int = 0, count: int = 4096) -> dict:
     return {"ma": ma.astype(np.float32), "ms": ms.astype(np.float32),
             "g": g.astype(np.float32), "n": n.astype(np.float32),
             "thickness": th.astype(np.float32), "n_photons": nph, "n_ambient": 1.0}
+
+
+SKIN_LAYERS = [(0.5, 20.0, 0.8, 1.4, 0.1), (0.05, 15.0, 0.85, 1.4, 1.5),
+               (0.02, 10.0, 0.9, 1.44, 1.4)]   # (ma, ms, g, n, thickness)
+
+
+def skin_stack_sweep(seed: int = 0, count: int = 1024) -> dict:
+    """A parameter sweep of three-layer skin stacks, as the reference's
+    dataset driver sweeps PlateModel optics (pymopt/virtualOBD.py:139-147):
+    the layers of the C2 slab (epidermis 0.1 mm, dermis 1.5 mm, subcutis
+    1.4 mm), each layer's mu_a scaled by a log-uniform factor in [1/2, 2] and
+    mu_s by one in [e^-0.5, e^0.5], photon budgets log-uniform in [1e4, 1e5].
+    Returns ``stacks`` (count x 3 layer tuples) and ``n_photons``."""
+    rng = _rng(seed)
+    fa = np.exp(rng.uniform(-np.log(2.0), np.log(2.0), (count, 3)))
+    fs = np.exp(rng.uniform(-0.5, 0.5, (count, 3)))
+    stacks = [[(ma * fa[i, j], ms * fs[i, j], g, n, t)
+               for j, (ma, ms, g, n, t) in enumerate(SKIN_LAYERS)] for i in range(count)]
+    photons = np.exp(rng.uniform(np.log(1e4), np.log(1e5), count)).astype(np.int64)
+    return {"stacks": stacks, "n_photons": photons}
+

@@ -161,3 +161,23 @@ def test_stack_ledger_completion_graph_and_bad_stack(cuda):
     r = st.run(use_graph=False)
     S = r["sums"][0]
     assert S[A.PMO_SS_ERRW] == photons[0] and S[A.PMO_SS_RD] == 0
+
+
+def test_stack_sweep_against_plain_comparator(cuda):
+    """The bench's layered leg on a small sweep: the batch and the reused
+    plain comparator both run, the batch closes its ledger, and on the sweep's
+    first problem the plain path's Rd agrees with the stack's within the
+    difference a 20 mm wide plate makes (lateral escape) plus noise."""
+    from pymonteopt_b200 import volumes as V
+    out = B.stacks_vs_plain(count=32, plain_sample=4, device=cuda)
+    assert out["problems"] == 32 and out["ratio"] > 0
+    assert out["max_energy_residual"] < 1e-9
+    sw = V.skin_stack_sweep(seed=0, count=32)
+    layers, N = sw["stacks"][0], 400000
+    ev = B.PlainStackEvaluator(V.SKIN_LAYERS, N, device=cuda)
+    plain = ev.evaluate(layers, N, 7)
+    stack = B.StackBatch([layers], N, seed=7, nr=0).run(use_graph=False)
+    assert abs(plain["Rd"] - stack["Rd"][0]) < 0.01, (plain["Rd"], stack["Rd"][0])
+    for li in range(3):
+        a, b = plain["dR_dma"][li], stack["dRd_dma"][0, li]
+        assert np.sign(a) == np.sign(b) and abs(a - b) <= 0.1 * abs(b) + 1e-3, (li, a, b)
