@@ -473,7 +473,6 @@ class BaseVoxelMonteCarlo(metaclass=ABCMeta):
         self.device = device
         self._dprob = None
         self._dprob_key = None
-        self._labels_at_upload = None
         self._tallies = None
         self.Rdw = self.Ttw = None
         self._reset_results()
@@ -553,22 +552,30 @@ class BaseVoxelMonteCarlo(metaclass=ABCMeta):
 
     # ---- run ---------------------------------------------------------------
     def _device_problem(self):
-        """The resident volume of this model, uploaded again (with its box
-        map) whenever the model was rebuilt or its labels or optics changed.
-        The label volume is snapshotted at upload, so an in-place edit of
-        ``model.voxel_model`` between two starts is seen too."""
+        """The resident volume of this model.  A rebuilt model, or changed
+        optical tables, get a fresh upload with its box map.  Otherwise the
+        labels are uploaded again, as the reference's start() does
+        (pymopt/voxel_gpu/_classes.py:92-101), and compared with the resident
+        copy on the device, so that an in-place edit of ``model.voxel_model``
+        between two starts replaces the volume and rebuilds the box map."""
+        import torch
         from . import engine as E
         prob = self.transport_problem()
         key = (id(self.model.voxel_model), prob.labels.shape, prob.ma.tobytes(),
                prob.ms.tobytes(), prob.g.tobytes(), prob.n.tobytes())
-        if self._dprob is None or self._dprob_key != key or \
-                not np.array_equal(self._labels_at_upload, prob.labels):
+        if self._dprob is None or self._dprob_key != key:
             self._dprob = E.DeviceProblem(prob, self.device)
             self._dprob_key = key
-            self._labels_at_upload = prob.labels.copy()
-        else:
-            self._dprob.host = prob  # source may have changed (beam settings)
-        return self._dprob
+            return self._dprob
+        dp = self._dprob
+        fresh = torch.from_numpy(prob.labels).to(dp.device)
+        if not torch.equal(fresh, dp.labels):
+            prob.validate()
+            dp.labels.copy_(fresh)
+            if dp.words is not None:
+                dp.build_words()
+        dp.host = prob  # the source may have changed too (beam settings)
+        return dp
 
     def start(self, rand_seed=None):
         from . import engine as E

@@ -159,3 +159,25 @@ def test_label_without_optics_is_reported(cuda):
         t.check()
     assert err.value.status == A.PMO_ERR_LABEL
     assert t.host_counters()[A.PMO_C_ERR_LABEL] > 0
+
+
+def test_model_start_sees_in_place_volume_edit(cuda):
+    """start() uploads the labels again and compares them with the resident
+    copy on the device: an in-place edit of model.voxel_model between two
+    starts takes effect (box map rebuilt), an unchanged volume stays."""
+    from pymonteopt_b200 import VoxelPlateModel
+    m = VoxelPlateModel(nPh=50000, keep_exits=False, verbose=False, device=cuda)
+    m.build(x_size=3.0, y_size=3.0, voxel_space=0.1, thickness=[0.5, 1.0], n=[1.4, 1.4],
+            n_air=1.0, ma=[0.1, 2.0], ms=[10.0, 10.0], g=[0.9, 0.9])
+    rd0 = m.start(5).getRdTtValues()["Rd"]
+    dp0 = m._dprob
+    assert m.start(5).getRdTtValues()["Rd"] == rd0 and m._dprob is dp0
+    # turn the strongly absorbing second layer into the first layer's tissue
+    vm = m.model.voxel_model
+    vm[vm == 1] = 0
+    rd1 = m.start(5).getRdTtValues()["Rd"]
+    assert m._dprob is dp0 and rd1 > rd0 + 0.01, (rd0, rd1)
+    lab = m._dprob.labels.cpu().numpy()
+    assert np.array_equal(lab, vm.view(np.uint8))
+    words = m._dprob.words.cpu().numpy().view(np.uint16)
+    assert np.array_equal(words & 0xff, lab)
