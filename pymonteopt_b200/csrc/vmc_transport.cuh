@@ -237,8 +237,6 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
     const bool photon_stats = (kp.flags & PMO_FLAG_PHOTON_STATS) != 0;
     const bool score_record = !GRAD && (kp.flags & PMO_FLAG_SCORE_RECORD) != 0;
 
-    // thread totals, reduced once at the end
-    double t_abs = 0.0;
 
     // photon state (registers).  The photon sits in a label-uniform box
     // {|dx|, |dy| <= bl, |dz| <= bz} (voxels) around voxel (ix, iy, iz) with
@@ -375,7 +373,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
     // photon end: per-photon outputs and counters
     // code: the exit's R(r) bin code (category * nr + bin), -1 for none
     auto finish = [&](int code = -1) {
-        t_abs += (double)wseg - (double)w;
+        atomicAdd(s_led + PMO_L_ABS, (double)wseg - (double)w);
         wseg = w;
         if (FLU != PMO_FLU_NONE) deposit_flush();
         // a replayed photon that ends without a binned exit left the forward path
@@ -833,7 +831,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
         // or the draw (k - 1, 3, photon) when a Fresnel decision took it
         if (w <= R(0.0001)) {
             atomicAdd(s_cnt + PMO_C_ROULETTE, 1ull);
-            t_abs += (double)wseg - (double)w;
+            atomicAdd(s_led + PMO_L_ABS, (double)wseg - (double)w);
             uint32_t word = ry;
             if (!ry_free) {
                 word = philox4x32_10(make_uint4(k - 1u, 3u, (uint32_t)pid, (uint32_t)(pid >> 32)),
@@ -917,14 +915,7 @@ __global__ void __launch_bounds__(512) vmc_plain_kernel(const KParams kp) {
         if (active) active = cycle(act);
     }
 
-    // ---- block epilogue: reduce thread totals, flush privatised tallies ----
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        t_abs += __shfl_xor_sync(FULL, t_abs, o);
-    }
-    if (lane == 0) {
-        atomicAdd(s_led + PMO_L_ABS, t_abs);
-    }
+    // ---- block epilogue: flush the privatised tallies ----
     __syncthreads();
     for (int i = threadIdx.x; i < PMO_LEDGER_N; i += blockDim.x)
         if (s_led[i] != 0.0) atomicAdd(kp.ledger + i, s_led[i]);

@@ -49,7 +49,11 @@ def test_one_layer_stack_follows_slab_batch(cuda, precision):
     np.testing.assert_allclose(got["dRd_dma"][:, 0], ref["dRd_dma"], rtol=1e-9)
     np.testing.assert_allclose(got["dTt_dms"][:, 0], ref["dTt_dms"], rtol=1e-9, atol=1e-12)
     np.testing.assert_allclose(got["Rr"], ref["Rr"], rtol=1e-5, atol=1e-9)
-    np.testing.assert_allclose(got["dRr_dms"][:, :, 0], ref["dRr_dms"], rtol=1e-4, atol=1e-8)
+    # per-bin derivatives are differences of two float32 atomic sums: compare
+    # them against the size of the profile
+    for col in ("dRr_dma", "dRr_dms"):
+        scale = np.abs(ref[col]).max(axis=1, keepdims=True)
+        assert np.all(np.abs(got[col][:, :, 0] - ref[col]) <= 1e-4 * scale), col
 
 
 def test_three_layer_stack_matches_reference(cuda):
@@ -176,8 +180,9 @@ def test_stack_sweep_against_plain_comparator(cuda):
     layers, N = sw["stacks"][0], 400000
     ev = B.PlainStackEvaluator(V.SKIN_LAYERS, N, device=cuda)
     plain = ev.evaluate(layers, N, 7)
-    stack = B.StackBatch([layers], N, seed=7, nr=0).run(use_graph=False)
+    stack = B.StackBatch([layers], N, seed=7, nr=32, dr=0.1).run(use_graph=False)
     assert abs(plain["Rd"] - stack["Rd"][0]) < 0.01, (plain["Rd"], stack["Rd"][0])
+    # both are derivatives of the sum of the 32 R(r) bins
     for li in range(3):
-        a, b = plain["dR_dma"][li], stack["dRd_dma"][0, li]
+        a, b = plain["dR_dma"][li], float(stack["dRr_dma"][0, :, li].sum())
         assert np.sign(a) == np.sign(b) and abs(a - b) <= 0.1 * abs(b) + 1e-3, (li, a, b)
