@@ -290,7 +290,7 @@ class StackBatch:
 
     def __init__(self, stacks, photons, *, n_ambient=1.0, nr: int = 32, dr: float = 0.1,
                  seed: int = 0, precision: int = A.PMO_FP32, device=None,
-                 block_threads: int = 128, chunk: int = 256):
+                 block_threads: int = 0, chunk: int = 0, autotune: bool = False):
         load()
         self.device = E.require_cuda(device)
         P = len(stacks)
@@ -316,7 +316,6 @@ class StackBatch:
         self.nr = int(nr)
         self.seed = int(seed)
         self.precision = precision
-        self.block_threads = int(block_threads)
         dev = self.device
         self.stacks = torch.from_numpy(st.view(np.uint8).copy()).to(dev)
         self.layers = torch.from_numpy(table.view(np.uint8).copy()).to(dev)
@@ -329,17 +328,69 @@ class StackBatch:
         self.rr = torch.zeros(P, max(self.nr, 1), A.PMO_SB_N, dtype=torch.float64, device=dev)
         self.workspace = torch.zeros(int(load().pmo_workspace_bytes()), dtype=torch.uint8,
                                      device=dev)
+        self.photons = photons
+        self.graph = None
+        if autotune and not (block_threads and chunk):
+            block_threads, chunk = self.autotune(block_threads=block_threads, chunk=chunk)
+        self.block_threads = int(block_threads or 128)
+        self.set_chunk(chunk or 256)
+
+    def set_chunk(self, chunk: int) -> None:
         self.chunk = int(chunk)
-        items = build_items(photons, self.chunk)
-        self.items = torch.from_numpy(items.view(np.uint8).copy()).to(dev)
+        items = build_items(self.photons, self.chunk)
+        self.items = torch.from_numpy(items.view(np.uint8).copy()).to(self.device)
         self.n_items = len(items)
         self.graph = None
 
-    def _struct(self) -> A.PmoStackBatch:
+    def autotune(self, scale: float = 1 / 16, block_threads: int = 0, chunk: int = 0) -> tuple:
+        """Pick (threads per block, photons per work item) by timing the
+        candidates (64, 128, 256) x (64, 256, 1024) on a copy of the batch
+        with every budget scaled by ``scale``; cached per device and batch
+        signature.  Arguments that are set (non-zero) are kept as given."""
+        sig = ("stack", torch.cuda.get_device_name(self.device), self.P,
+               int(self.photons.sum()), len(self.host_layers),
+               round(float(self.host_layers["ma"].mean()), 6), block_threads, chunk)
+        if sig in _TUNE_CACHE:
+            self.tune_table = _TUNE_CACHE[sig]
+            return self.tune_table["best"]
+        cands = [(t, c) for t in ((block_threads,) if block_threads else (64, 128, 256))
+                 for c in ((chunk,) if chunk else (64, 256, 1024))]
+        small = np.maximum(1, (self.photons * scale).astype(np.int64))
+        st = self.host_stacks.copy()
+        st["photons"] = small
+        d_st = torch.from_numpy(st.view(np.uint8).copy()).to(self.device)
+        lib = load()
+        times = {}
+        for t, c in cands:
+            items = build_items(small, c)
+            d_items = torch.from_numpy(items.view(np.uint8).copy()).to(self.device)
+            b = self._struct(stacks=d_st, items=d_items, n_items=len(items))
+            best = float("inf")
+            for rep in range(3):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record()
+                check(lib.pmo_run_stack_batch(C.byref(b), C.byref(A.PmoLaunch(t, 0)),
+                                              C.c_void_p(self.workspace.data_ptr()),
+                                              self.workspace.numel(), E._stream_handle()),
+                      "pmo_run_stack_batch (autotune)")
+                e1.record()
+                torch.cuda.synchronize()
+                if rep:
+                    best = min(best, e0.elapsed_time(e1))
+            times[(t, c)] = best
+        choice = min(times, key=times.get)
+        self.tune_table = {"best": choice, "ms": {f"{t}x{c}": v for (t, c), v in times.items()},
+                           "scale": scale}
+        _TUNE_CACHE[sig] = self.tune_table
+        return choice
+
+    def _struct(self, stacks=None, items=None, n_items=None) -> A.PmoStackBatch:
         b = A.PmoStackBatch()
-        b.stacks, b.n_problems = self.stacks.data_ptr(), self.P
+        b.stacks = (stacks if stacks is not None else self.stacks).data_ptr()
+        b.n_problems = self.P
         b.layers, b.n_layer_rows = self.layers.data_ptr(), len(self.host_layers)
-        b.items, b.n_items = self.items.data_ptr(), self.n_items
+        b.items = (items if items is not None else self.items).data_ptr()
+        b.n_items = n_items if n_items is not None else self.n_items
         b.seed = self.seed & 0xFFFFFFFFFFFFFFFF
         b.nr = self.nr
         b.sums, b.bins = self.sums.data_ptr(), self.bins.data_ptr()
@@ -678,7 +729,9 @@ def stacks_vs_plain(count: int = 1024, plain_sample: int = 48, seed: int = 0, nr
     from . import volumes as V
     sw = V.skin_stack_sweep(seed=seed, count=count)
     stacks, photons = sw["stacks"], sw["n_photons"]
-    sb = StackBatch(stacks, photons, nr=nr, dr=dr, seed=seed + 1, device=device)
+    t0 = time.perf_counter()
+    sb = StackBatch(stacks, photons, nr=nr, dr=dr, seed=seed + 1, device=device, autotune=True)
+    tune_s = time.perf_counter() - t0
     sb.capture()
     tb = time_batch(sb, reps=3)
     res = sb.fetch()
@@ -702,6 +755,8 @@ def stacks_vs_plain(count: int = 1024, plain_sample: int = 48, seed: int = 0, nr
         "plain_evals_per_s": plain_rate,
         "plain_path": "PlainStackEvaluator: one resident 20 x 20 mm plate at 0.05 mm, optics "
                       "rewritten per problem, scored forward + per-label replay + read-back",
+        "launch_shape": {"block_threads": sb.block_threads, "photons_per_item": sb.chunk},
+        "autotune_seconds": tune_s,
         "plain_sample": len(pick), "ratio": tb["evals_per_s"] / plain_rate,
         "p50_completion_ms": float(np.percentile(comp, 50)),
         "p99_completion_ms": float(np.percentile(comp, 99)),

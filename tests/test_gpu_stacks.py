@@ -186,3 +186,16 @@ def test_stack_sweep_against_plain_comparator(cuda):
     for li in range(3):
         a, b = plain["dR_dma"][li], float(stack["dRr_dma"][0, :, li].sum())
         assert np.sign(a) == np.sign(b) and abs(a - b) <= 0.1 * abs(b) + 1e-3, (li, a, b)
+
+
+def test_stack_autotuner_picks_a_shape_and_shapes_agree(cuda):
+    """The launch shape changes neither the photons nor the results."""
+    sw = V.skin_stack_sweep(seed=4, count=24)
+    photons = np.maximum(2000, sw["n_photons"] // 10)
+    tuned = B.StackBatch(sw["stacks"], photons, nr=16, dr=0.1, seed=8, autotune=True)
+    assert (tuned.block_threads, tuned.chunk) == tuned.tune_table["best"]
+    assert len(tuned.tune_table["ms"]) == 9
+    fixed = B.StackBatch(sw["stacks"], photons, nr=16, dr=0.1, seed=8, block_threads=64,
+                         chunk=1024)
+    a, b = tuned.run(use_graph=False), fixed.run(use_graph=False)
+    np.testing.assert_allclose(a["sums"], b["sums"], rtol=1e-10, atol=1e-10)
