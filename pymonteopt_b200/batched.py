@@ -766,7 +766,8 @@ def stacks_vs_plain(count: int = 1024, plain_sample: int = 48, seed: int = 0, nr
 
 def main(argv=None) -> int:
     """``python -m pymonteopt_b200.batched``: time graph replays of the C5
-    slab batch (forward + gradient) and print one JSON line."""
+    slab batch (forward + gradient), or with ``--stacks`` of the layered skin
+    sweep, and print one JSON line."""
     import argparse
     import json
     from . import volumes as V
@@ -779,7 +780,25 @@ def main(argv=None) -> int:
     ap.add_argument("--chunk", type=int, default=0, help="photons per work item")
     ap.add_argument("--tally-mode", choices=["auto", "thread", "global"], default="auto",
                     help="per-problem sums privatised per thread, or straight to global memory")
+    ap.add_argument("--stacks", action="store_true",
+                    help="the layered batch on the skin sweep (volumes.skin_stack_sweep) instead")
     args = ap.parse_args(argv)
+    if args.stacks:
+        sw = V.skin_stack_sweep(seed=0, count=args.count)
+        photons = np.maximum(1, (sw["n_photons"] * args.photon_scale).astype(np.int64))
+        st = StackBatch(sw["stacks"], photons, nr=32, dr=0.1, seed=1,
+                        block_threads=args.block_threads, chunk=args.chunk, autotune=True)
+        tb = time_batch(st, reps=args.reps)
+        res = st.fetch()
+        print(json.dumps({"problems": st.P, "layers_per_problem": 3,
+                          "photons": float(photons.sum()), "seconds": tb["seconds"],
+                          "evals_per_s": tb["evals_per_s"],
+                          "photons_per_s": float(photons.sum()) / tb["seconds"],
+                          "block_threads": st.block_threads, "photons_per_item": st.chunk,
+                          "autotune": getattr(st, "tune_table", None),
+                          "p99_completion_ms": float(np.percentile(res["completion_ms"], 99)),
+                          "max_energy_residual": float(np.max(np.abs(res["balance"])))}))
+        return 0
     b = V.c5_slab_batch(seed=0, count=args.count)
     photons = np.maximum(1, (b["n_photons"] * args.photon_scale).astype(np.int64))
     mode = {"auto": None, "thread": A.PMO_BT_THREAD, "global": A.PMO_BT_GLOBAL}[args.tally_mode]
