@@ -596,14 +596,33 @@ def fp32_probe(torch, lib) -> float:
     return best
 
 
+# the sources that define the plain transport kernel's instructions; the ncu
+# summary records their digest, and figures captured from other sources are
+# not used
+KERNEL_SOURCES = ("vmc_transport.cuh", "philox.cuh", "pmo_internal.h")
+
+
+def kernel_source_digest() -> str:
+    import hashlib
+    h = hashlib.sha256()
+    for name in KERNEL_SOURCES:
+        with open(os.path.join(REPO, "pymonteopt_b200", "csrc", name), "rb") as f:
+            h.update(f.read())
+    return h.hexdigest()
+
+
 def read_traffic():
-    """DRAM bytes per photon of the transport kernel from the committed ncu
-    summary, if present."""
+    """DRAM bytes and instructions per photon of the transport kernel from the
+    committed ncu summary, if present and captured from the current kernel
+    sources; else None (the line then carries no traffic)."""
     path = os.path.join(REPO, "profiles", "vmc_plain_c2_ncu.json")
     if not os.path.exists(path):
         return None
     with open(path) as f:
-        return json.load(f)
+        d = json.load(f)
+    if d.get("kernel_source_sha256") != kernel_source_digest():
+        return None
+    return d
 
 
 def summary_dict(value, e2e, parity, batched, gradient, reference_gpu, cpu, roofline,
@@ -719,6 +738,8 @@ def main() -> int:
         "frac": achieved / peak,
         "peak_source": "measured in this run: FFMA-throughput probe (pmo_fp32_probe)",
         "traffic": (traffic["dram_bytes_per_photon"] * photons) if traffic else None,
+        "traffic_note": None if traffic else
+            "no ncu summary captured from the current kernel sources",
         "traffic_unit": "bytes per launch (ncu dram__bytes_read+write, scaled per photon)",
         "algorithmic_fp32_per_photon": fp32_per_launch / photons,
         "mufu_per_photon": opcount.mufu_ops(counters.astype(np.uint64)) / (photons * args.steps),
