@@ -575,9 +575,10 @@ int pmo_fp32_probe(float *out, int blocks, int threads, int iters, void *stream)
      lat(c) = ((2 | (c & 1)) << (c >> 1)) >> 1 (1, 2, 3, 4, 6, ... 192);
    - c is the largest code whose lat(c) does not exceed the smallest
      in-plane uniform radius over the box's z-planes.
-   scratch: 3 * nx*ny*nz bytes of device memory.  No counterpart in the
-   reference, which steps voxel by voxel
-   (pymopt/voxel_gpu/_cukernel.py:77-176). */
+   scratch: PMO_VOXEL_WORDS_SCRATCH * nx*ny*nz bytes of device memory,
+   4-byte aligned; nx*ny*nz < 2^32.  No counterpart in the reference, which
+   steps voxel by voxel (pymopt/voxel_gpu/_cukernel.py:77-176). */
+#define PMO_VOXEL_WORDS_SCRATCH 5   /* scratch bytes per voxel */
 int pmo_build_voxel_words(const uint8_t *labels, int nx, int ny, int nz, int cap,
                           uint16_t *words, void *scratch, size_t scratch_bytes,
                           void *stream);

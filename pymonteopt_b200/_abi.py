@@ -81,6 +81,7 @@ PMO_FD_MAX = 32
 
 PMO_WS_LEDGER_OFFSET = 64
 PMO_STATIC_WORKSPACE_BYTES = 512
+PMO_VOXEL_WORDS_SCRATCH = 5
 PMO_WS_COUNTERS_OFFSET = 256
 
 STATUS_NAMES = {

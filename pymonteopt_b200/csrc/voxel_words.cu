@@ -17,130 +17,205 @@
 // L-infinity distance to the edge set E (voxels with a 26-neighbour of another
 // label, and the array border).  If a voxel w of another label were within
 // distance D_E(v) of v, the voxel next to w on the way from v would be in E and
-// closer than D_E(v).  The transform is separable:
-// D(v) = min over |k| <= cap of max(|k|, D_prev(v + k e_axis)), one pass per
-// axis, the first pass starting from 0 on E and "infinity" elsewhere.
+// closer than D_E(v).
 //
 // e: P(u), the same construction inside u's z-plane with the 8 in-plane
-// neighbours and the lateral border (two passes, x and y, capped at 192), is
-// the half-extent of a uniform in-plane square around u.  The box's slices
-// are the squares around v + dz*z_hat for |dz| <= d, which lie in v's cube and
-// so carry label(v).  Hence e_true = min over |dz| <= d of P(v + dz*z_hat), and
-// e_true >= d.  The word stores the largest code with lat(c) <= e_true.  This
-// widens the boxes of thin layers, such as a 2-voxel skin layer whose voxels
-// all have d = 0.
+// neighbours and the lateral border (capped at 192), is the half-extent of a
+// uniform in-plane square around u.  The box's slices are the squares around
+// v + dz*z_hat for |dz| <= d, which lie in v's cube and so carry label(v).
+// Hence e_true = min over |dz| <= d of P(v + dz*z_hat), and e_true >= d.  The
+// word stores the largest code with lat(c) <= e_true.  This widens the boxes
+// of thin layers, such as a 2-voxel skin layer whose voxels all have d = 0.
+//
+// Both are found by counting edge voxels in boxes.  D_E(v) >= r exactly when
+// the cube of half-extent r - 1 around v holds no voxel of E (clipped to the
+// array: a cube that reaches past it holds border voxels, which are in E), so
+// d is the largest r <= cap whose cube count is zero.  Likewise lat(c) <=
+// e_true exactly when the box of half-extents (lat(c) - 1, lat(c) - 1, d)
+// holds no voxel of E2 (the in-plane edge set), so c is the largest code
+// whose box count is zero.  Both counts fall as the box shrinks, so a binary
+// search over r (0 .. 15) and over c (0 .. 15) takes four box counts each.  A
+// box count is eight reads of a summed-area table (inclusive 3-D prefix sums
+// of the edge indicator), kept as uint32: the counts are exact modulo 2^32
+// and no box holds 2^32 voxels.
+//
+// Passes (each streams the volume once, coalesced along z):
+//   1. edges + z prefix: one warp per (x, y) row; the E and E2 bits of each
+//      voxel into the mask byte, the warp-scanned z prefix of E into the table;
+//   2. y prefix, 3. x prefix: one thread per row, a running sum;
+//   4. d per voxel (binary search on the table of E), into the mask byte;
+//   5-7. the table again, for E2;
+//   8. c per voxel (binary search on the table of E2) and the word.
 #include "pmo_internal.h"
 
 namespace {
 
-constexpr uint8_t kInf = 255;
-constexpr int kLatCap = 192;   // lat(15)
+constexpr unsigned kFull = 0xffffffffu;
 
 __host__ __device__ inline int lat_of(int c) {
     return c ? ((2 | (c & 1)) << (c >> 1)) >> 1 : 0;
 }
 
-// E: 0 where a 26-neighbour (inside the array) has another label, else kInf.
-__global__ void edge_kernel(const uint8_t *__restrict__ lab, int nx, int ny, int nz,
-                            uint8_t *__restrict__ out) {
-    const uint64_t total = (uint64_t)nx * ny * nz;
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
-         i += (uint64_t)gridDim.x * blockDim.x) {
-        const int z = (int)(i % nz);
-        const int y = (int)((i / nz) % ny);
-        const int x = (int)(i / ((uint64_t)nz * ny));
-        const uint8_t me = lab[i];
-        bool edge = false;
-        for (int dx = -1; dx <= 1 && !edge; ++dx) {
-            const int xx = x + dx;
-            if (xx < 0 || xx >= nx) continue;
-            for (int dy = -1; dy <= 1 && !edge; ++dy) {
-                const int yy = y + dy;
-                if (yy < 0 || yy >= ny) continue;
-                const uint64_t row = ((uint64_t)xx * ny + yy) * nz;
-                for (int dz = -1; dz <= 1; ++dz) {
-                    const int zz = z + dz;
-                    if (zz < 0 || zz >= nz) continue;
-                    if (lab[row + zz] != me) { edge = true; break; }
+// Pass 1.  mask = E | E2 << 1; sat = prefix of E along z.  One warp per
+// (x, y) row; the row index is warp-uniform, so are the loop bounds.
+__global__ void edge_scan_z_kernel(const uint8_t *__restrict__ lab, int nx, int ny, int nz,
+                                   uint8_t *__restrict__ mask, uint32_t *__restrict__ sat) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t rows = (uint32_t)nx * (uint32_t)ny;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < rows; row += warps) {
+        const int x = (int)(row / (uint32_t)ny), y = (int)(row % (uint32_t)ny);
+        const bool lateral = x == 0 || y == 0 || x == nx - 1 || y == ny - 1;
+        const size_t base = (size_t)row * nz;
+        uint32_t carry = 0;
+        for (int z0 = 0; z0 < nz; z0 += 32) {
+            const int z = z0 + lane;
+            uint32_t e = 0, e2 = 0;
+            if (z < nz) {
+                if (lateral) {
+                    e = e2 = 1;
+                } else {
+                    // interior row: the 8 neighbouring rows exist
+                    const uint8_t me = lab[base + z];
+                    uint32_t plane = 0, off = 0;
+                    for (int dx = -1; dx <= 1; ++dx) {
+                        for (int dy = -1; dy <= 1; ++dy) {
+                            const uint8_t *r = lab + (size_t)((ptrdiff_t)base +
+                                                              ((ptrdiff_t)dx * ny + dy) * nz);
+                            plane |= r[z] != me;
+                            if (z > 0) off |= r[z - 1] != me;
+                            if (z < nz - 1) off |= r[z + 1] != me;
+                        }
+                    }
+                    e2 = plane;
+                    e = plane | off | (z == 0) | (z == nz - 1);
                 }
+                mask[base + z] = (uint8_t)(e | (e2 << 1));
             }
+            uint32_t s = e;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(kFull, s, o);
+                if (lane >= o) s += t;
+            }
+            if (z < nz) sat[base + z] = carry + s;
+            carry += __shfl_sync(kFull, s, 31);
         }
-        // the array border counts as an edge: boxes never reach past it
-        if (x == 0 || y == 0 || z == 0 || x == nx - 1 || y == ny - 1 || z == nz - 1) edge = true;
-        out[i] = edge ? 0 : kInf;
     }
 }
 
-// E2: 0 where an in-plane 8-neighbour has another label, or on the lateral
-// array border; else kInf.
-__global__ void edge2_kernel(const uint8_t *__restrict__ lab, int nx, int ny, int nz,
-                             uint8_t *__restrict__ out) {
-    const uint64_t total = (uint64_t)nx * ny * nz;
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
-         i += (uint64_t)gridDim.x * blockDim.x) {
-        const int z = (int)(i % nz);
-        const int y = (int)((i / nz) % ny);
-        const int x = (int)(i / ((uint64_t)nz * ny));
-        const uint8_t me = lab[i];
-        bool edge = x == 0 || y == 0 || x == nx - 1 || y == ny - 1;
-        for (int dx = -1; dx <= 1 && !edge; ++dx) {
-            for (int dy = -1; dy <= 1; ++dy) {
-                if (lab[((uint64_t)(x + dx) * ny + (y + dy)) * nz + z] != me) {
-                    edge = true;
-                    break;
-                }
+// Pass 5.  sat = prefix along z of bit `bit` of the mask.
+__global__ void scan_z_bit_kernel(const uint8_t *__restrict__ mask, int nx, int ny, int nz,
+                                  int bit, uint32_t *__restrict__ sat) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t rows = (uint32_t)nx * (uint32_t)ny;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < rows; row += warps) {
+        const size_t base = (size_t)row * nz;
+        uint32_t carry = 0;
+        for (int z0 = 0; z0 < nz; z0 += 32) {
+            const int z = z0 + lane;
+            uint32_t s = z < nz ? (mask[base + z] >> bit) & 1u : 0u;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(kFull, s, o);
+                if (lane >= o) s += t;
             }
+            if (z < nz) sat[base + z] = carry + s;
+            carry += __shfl_sync(kFull, s, 31);
         }
-        out[i] = edge ? 0 : kInf;
     }
 }
 
-// One separable pass of the L-infinity distance transform along `axis`.
-__global__ void dt_pass_kernel(const uint8_t *__restrict__ in, int nx, int ny, int nz, int axis,
-                               int cap, uint8_t *__restrict__ out) {
-    const uint64_t total = (uint64_t)nx * ny * nz;
-    const int dim = axis == 0 ? nx : (axis == 1 ? ny : nz);
-    const uint64_t stride = axis == 0 ? (uint64_t)ny * nz : (axis == 1 ? (uint64_t)nz : 1);
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
-         i += (uint64_t)gridDim.x * blockDim.x) {
-        const int c = axis == 0 ? (int)(i / ((uint64_t)nz * ny))
-                                : (axis == 1 ? (int)((i / nz) % ny) : (int)(i % nz));
-        int best = in[i];
-        for (int k = 1; k <= cap && k < best; ++k) {
-            if (c - k >= 0) {
-                const int v = in[i - k * stride];
-                const int m = v > k ? v : k;
-                if (m < best) best = m;
-            }
-            if (c + k < dim) {
-                const int v = in[i + k * stride];
-                const int m = v > k ? v : k;
-                if (m < best) best = m;
+// Passes 2 and 3.  In-place running sum along y (stride nz) or x (stride
+// ny*nz); one thread per row, consecutive threads on consecutive z.  Eight
+// loads are issued before their sums are stored.
+__global__ void scan_strided_kernel(uint32_t *__restrict__ sat, uint32_t rows, int nz,
+                                    size_t outer_stride, size_t stride, int len) {
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < rows;
+         t += gridDim.x * blockDim.x) {
+        uint32_t *p = sat + (size_t)(t / (uint32_t)nz) * outer_stride + (t % (uint32_t)nz);
+        uint32_t run = 0;
+        int k = 0;
+        for (; k + 8 <= len; k += 8) {
+            uint32_t v[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) v[j] = p[(size_t)(k + j) * stride];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                run += v[j];
+                p[(size_t)(k + j) * stride] = run;
             }
         }
-        out[i] = (uint8_t)best;
+        for (; k < len; ++k) {
+            run += p[(size_t)k * stride];
+            p[(size_t)k * stride] = run;
+        }
     }
 }
 
-// words from the labels, the cube half-extent map dmap and the in-plane
-// radius map pmap
-__global__ void pack_kernel(const uint8_t *__restrict__ lab, const uint8_t *__restrict__ dmap,
-                            const uint8_t *__restrict__ pmap, int nz, uint64_t total, int cap,
+struct Grid3 {
+    int nx, ny, nz;
+};
+
+__device__ inline uint32_t sat_at(const uint32_t *__restrict__ s, const Grid3 &g, int x, int y,
+                                  int z) {
+    return (x < 0 || y < 0 || z < 0) ? 0u : __ldg(s + ((size_t)x * g.ny + y) * g.nz + z);
+}
+
+// edge voxels in [x-h, x+h] x [y-h, y+h] x [z-hz, z+hz], clipped to the array
+__device__ inline uint32_t box_count(const uint32_t *__restrict__ s, const Grid3 &g, int x, int y,
+                                     int z, int h, int hz) {
+    const int xa = max(x - h, 0) - 1, xb = min(x + h, g.nx - 1);
+    const int ya = max(y - h, 0) - 1, yb = min(y + h, g.ny - 1);
+    const int za = max(z - hz, 0) - 1, zb = min(z + hz, g.nz - 1);
+    return sat_at(s, g, xb, yb, zb) - sat_at(s, g, xa, yb, zb) - sat_at(s, g, xb, ya, zb) -
+           sat_at(s, g, xb, yb, za) + sat_at(s, g, xa, ya, zb) + sat_at(s, g, xa, yb, za) +
+           sat_at(s, g, xb, ya, za) - sat_at(s, g, xa, ya, za);
+}
+
+// Pass 4.  d into bits 2-5 of the mask.
+__global__ void depth_kernel(const uint32_t *__restrict__ sat, Grid3 g, uint32_t total, int cap,
+                             uint8_t *__restrict__ mask) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += gridDim.x * blockDim.x) {
+        const uint8_t m = mask[i];
+        int d = 0;
+        if (!(m & 1) && cap > 0) {
+            const int z = (int)(i % (uint32_t)g.nz);
+            const uint32_t row = i / (uint32_t)g.nz;
+            const int y = (int)(row % (uint32_t)g.ny), x = (int)(row / (uint32_t)g.ny);
+            int lo = 1, hi = cap + 1;   // r = lo is uniform (v is not in E), r = hi is not tested
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (box_count(sat, g, x, y, z, mid - 1, mid - 1) == 0u) lo = mid;
+                else hi = mid;
+            }
+            d = lo;
+        }
+        mask[i] = (uint8_t)((m & 3) | (d << 2));
+    }
+}
+
+// Pass 8.  The lateral code and the word.
+__global__ void pack_kernel(const uint8_t *__restrict__ lab, const uint8_t *__restrict__ mask,
+                            const uint32_t *__restrict__ sat, Grid3 g, uint32_t total,
                             uint16_t *__restrict__ words) {
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
-         i += (uint64_t)gridDim.x * blockDim.x) {
-        const int z = (int)(i % nz);
-        const int d = dmap[i] < cap ? dmap[i] : cap;
-        int e = kLatCap;
-        for (int dz = -d; dz <= d; ++dz) {
-            const int zz = z + dz;
-            if (zz < 0 || zz >= nz) { e = 0; break; }   // never with a valid d
-            const int p = pmap[(int64_t)i + dz];
-            if (p < e) e = p;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += gridDim.x * blockDim.x) {
+        const int d = (mask[i] >> 2) & 15;
+        int lo = 0, hi = 16;   // code 0 needs no uniform square
+        if (!(mask[i] & 2)) {
+            const int z = (int)(i % (uint32_t)g.nz);
+            const uint32_t row = i / (uint32_t)g.nz;
+            const int y = (int)(row % (uint32_t)g.ny), x = (int)(row / (uint32_t)g.ny);
+            while (hi - lo > 1) {
+                const int mid = (lo + hi) >> 1;
+                if (box_count(sat, g, x, y, z, lat_of(mid) - 1, d) == 0u) lo = mid;
+                else hi = mid;
+            }
         }
-        int c = 0;
-        while (c < 15 && lat_of(c + 1) <= e) ++c;
-        words[i] = (uint16_t)(lab[i] | (d << 8) | (c << 12));
+        words[i] = (uint16_t)(lab[i] | (d << 8) | (lo << 12));
     }
 }
 
@@ -148,30 +223,40 @@ __global__ void pack_kernel(const uint8_t *__restrict__ lab, const uint8_t *__re
 
 extern "C" {
 
-// words[nvox] (uint16) from labels[nvox]; scratch: 3 * nvox bytes.
+// words[nvox] (uint16) from labels[nvox]; scratch: PMO_VOXEL_WORDS_SCRATCH
+// bytes per voxel (the uint32 table, then the mask byte), 4-byte aligned.
 int pmo_build_voxel_words(const uint8_t *labels, int nx, int ny, int nz, int cap,
                           uint16_t *words, void *scratch, size_t scratch_bytes, void *stream) {
     if (!labels || !words || !scratch || nx < 1 || ny < 1 || nz < 1) return PMO_ERR_ARG;
     if (cap < 0 || cap > 15) return PMO_ERR_ARG;
     const uint64_t total = (uint64_t)nx * ny * nz;
-    if (scratch_bytes < 3 * total) return PMO_ERR_WORKSPACE;
+    if (total >= (1ull << 32)) return PMO_ERR_ARG;
+    if (reinterpret_cast<uintptr_t>(scratch) % 4 != 0) return PMO_ERR_ARG;
+    if (scratch_bytes < PMO_VOXEL_WORDS_SCRATCH * total) return PMO_ERR_WORKSPACE;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    uint8_t *a = static_cast<uint8_t *>(scratch);
-    uint8_t *b = a + total;
-    uint8_t *c = b + total;
-    uint64_t blocks = (total + 255) / 256;
-    if (blocks > 148ull * 64) blocks = 148ull * 64;
-    const unsigned g = (unsigned)blocks;
-    // d: 3-D distance to the edge set, capped
-    edge_kernel<<<g, 256, 0, s>>>(labels, nx, ny, nz, a);
-    dt_pass_kernel<<<g, 256, 0, s>>>(a, nx, ny, nz, 0, cap, b);
-    dt_pass_kernel<<<g, 256, 0, s>>>(b, nx, ny, nz, 1, cap, a);
-    dt_pass_kernel<<<g, 256, 0, s>>>(a, nx, ny, nz, 2, cap, b);
-    // P: in-plane distance to the in-plane edge set, capped at lat(15)
-    edge2_kernel<<<g, 256, 0, s>>>(labels, nx, ny, nz, a);
-    dt_pass_kernel<<<g, 256, 0, s>>>(a, nx, ny, nz, 0, kLatCap, c);
-    dt_pass_kernel<<<g, 256, 0, s>>>(c, nx, ny, nz, 1, kLatCap, a);
-    pack_kernel<<<g, 256, 0, s>>>(labels, b, a, nz, total, cap, words);
+    uint32_t *sat = static_cast<uint32_t *>(scratch);
+    uint8_t *mask = reinterpret_cast<uint8_t *>(sat + total);
+    const Grid3 g{nx, ny, nz};
+    const uint32_t n = (uint32_t)total;
+    auto blocks_for = [](uint64_t threads) {
+        uint64_t b = (threads + 255) / 256;
+        if (b > 148ull * 32) b = 148ull * 32;
+        return (unsigned)(b ? b : 1);
+    };
+    const unsigned g_rows = blocks_for((uint64_t)nx * ny * 32);   // a warp per (x, y) row
+    const unsigned g_vox = blocks_for(total);
+    const uint32_t rows_y = (uint32_t)nx * nz, rows_x = (uint32_t)ny * nz;
+    const size_t plane = (size_t)ny * nz;
+    // d: table of E, then the binary search
+    edge_scan_z_kernel<<<g_rows, 256, 0, s>>>(labels, nx, ny, nz, mask, sat);
+    scan_strided_kernel<<<blocks_for(rows_y), 256, 0, s>>>(sat, rows_y, nz, plane, nz, ny);
+    scan_strided_kernel<<<blocks_for(rows_x), 256, 0, s>>>(sat, rows_x, nz, nz, plane, nx);
+    depth_kernel<<<g_vox, 256, 0, s>>>(sat, g, n, cap, mask);
+    // c: table of E2, then the binary search and the words
+    scan_z_bit_kernel<<<g_rows, 256, 0, s>>>(mask, nx, ny, nz, 1, sat);
+    scan_strided_kernel<<<blocks_for(rows_y), 256, 0, s>>>(sat, rows_y, nz, plane, nz, ny);
+    scan_strided_kernel<<<blocks_for(rows_x), 256, 0, s>>>(sat, rows_x, nz, nz, plane, nx);
+    pack_kernel<<<g_vox, 256, 0, s>>>(labels, mask, sat, g, n, words);
     return cudaGetLastError() == cudaSuccess ? PMO_OK : PMO_ERR_CUDA;
 }
 

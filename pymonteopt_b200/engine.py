@@ -16,6 +16,7 @@ import torch
 
 from . import _abi as A
 from ._lib import PmoError, check, load
+from .problem import check_volume
 
 
 def _ptr(t: Optional[torch.Tensor]):
@@ -40,6 +41,19 @@ def require_cuda(device=None) -> torch.device:
 SKIP_CAP = 15   # z half-extent of the uniform boxes (lateral: up to 192 voxels)
 
 
+def check_labels(labels: torch.Tensor, end_label: int, n_labels: int) -> None:
+    """The volume checks of ``TransportProblem.validate`` (a complete shell of
+    ``end_label``, every label below ``n_labels``) on a device copy of the
+    labels: a few reductions and one read-back, instead of host passes over
+    the whole volume."""
+    e = int(end_label)
+    faces = (labels[0], labels[-1], labels[:, 0], labels[:, -1], labels[:, :, 0],
+             labels[:, :, -1])
+    shell = torch.stack([(f != e).any() for f in faces]).any()
+    flags = torch.stack([shell.to(torch.int32), labels.max().to(torch.int32)]).tolist()
+    check_volume(bool(flags[0]), int(flags[1]), int(n_labels))
+
+
 class DeviceProblem:
     """A problem whose volume and optical tables are resident on one GPU.
 
@@ -52,10 +66,11 @@ class DeviceProblem:
     def __init__(self, prob, device=None, *, skip: bool = True, skip_cap: int = SKIP_CAP):
         load()
         self.device = require_cuda(device)
-        prob.validate()
+        prob.validate(labels=False)
         self.host = prob
         dev = self.device
         self.labels = torch.from_numpy(prob.labels).to(dev)
+        check_labels(self.labels, prob.end_label, prob.n_labels)
         self.words = None
         self.skip_cap = int(skip_cap)
         if skip and prob.vox_ma is None:
@@ -74,7 +89,8 @@ class DeviceProblem:
 
     def build_words(self, stream=None) -> None:
         """(Re)build the uniform-box map from the resident labels."""
-        scratch = torch.empty(3 * self.labels.numel(), dtype=torch.uint8, device=self.device)
+        scratch = torch.empty(A.PMO_VOXEL_WORDS_SCRATCH * self.labels.numel(), dtype=torch.uint8,
+                              device=self.device)
         nx, ny, nz = self.labels.shape
         st = load().pmo_build_voxel_words(self.labels.data_ptr(), nx, ny, nz, self.skip_cap,
                                           self.words.data_ptr(), scratch.data_ptr(),

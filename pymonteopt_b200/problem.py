@@ -33,6 +33,16 @@ def center_add(length: int) -> int:
     return int((length - 1) / 2)
 
 
+def check_volume(shell_broken: bool, max_label: int, n_labels: int) -> None:
+    """Raise for a volume without a complete end_label shell, or with a label
+    that has no optical properties."""
+    if shell_broken:
+        raise ValueError("the volume must be enclosed by a one-voxel shell of end_label")
+    if max_label >= n_labels:
+        raise ValueError(f"label {max_label} has no optical properties "
+                         f"(n_labels = {n_labels})")
+
+
 @dataclass
 class TransportProblem:
     labels: np.ndarray                      # (nx, ny, nz) uint8, padded
@@ -89,12 +99,15 @@ class TransportProblem:
     def props_mode(self) -> int:
         return A.PMO_PROPS_VOXEL if self.vox_ma is not None else A.PMO_PROPS_LABEL
 
-    def validate(self) -> None:
+    def validate(self, labels: bool = True) -> None:
         """Host-side checks that the device kernels rely on.
 
         The reference never checks its volume; an unpadded volume would let
         cuVMC read outside ``voxel_model``.  Here the shell, the label range
-        and the source voxel are checked once per problem.
+        and the source voxel are checked once per problem.  ``labels=False``
+        leaves out the two checks that read the whole volume (the shell and
+        the label range); the engine runs those on the uploaded copy instead
+        (:func:`check_volume`).
         """
         lab = self.labels
         if lab.ndim != 3 or min(lab.shape) < 3:
@@ -105,12 +118,9 @@ class TransportProblem:
         if not (0 <= e < self.n_labels <= 256):
             raise ValueError(
                 f"end_label {e} must index n (len {self.n_labels}), n_labels <= 256")
-        faces = (lab[0], lab[-1], lab[:, 0], lab[:, -1], lab[:, :, 0], lab[:, :, -1])
-        if any(np.any(f != e) for f in faces):
-            raise ValueError("the volume must be enclosed by a one-voxel shell of end_label")
-        if int(lab.max()) >= self.n_labels:
-            raise ValueError(f"label {int(lab.max())} has no optical properties "
-                             f"(n_labels = {self.n_labels})")
+        if labels:
+            faces = (lab[0], lab[-1], lab[:, 0], lab[:, -1], lab[:, :, 0], lab[:, :, -1])
+            check_volume(any(np.any(f != e) for f in faces), int(lab.max()), self.n_labels)
         if self.voxel_space <= 0 or not np.isfinite(self.voxel_space):
             raise ValueError("voxel_space must be positive")
         for name in ("ma", "ms", "g", "n"):

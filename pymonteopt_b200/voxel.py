@@ -102,15 +102,26 @@ class PlateModel(VoxelModel):
         self._param_instantiating()
 
     def _make_voxel_model(self):
-        vm = np.empty((self.x_size + 2, self.y_size + 2, self.z_size + 2), dtype=self.dtype)
+        # every (x, y) column of the slab is the same: the layer labels along
+        # z between two shell voxels.  Writing that column across the plane is
+        # one contiguous pass over the volume; filling layer by layer
+        # (pymopt/voxel_gpu/_classes.py:437-457) writes short runs per column
+        # and takes about twice as long.  The bytes are the same, except that
+        # z voxels no layer reaches (rounded thicknesses that fall short of
+        # z_size) hold label 0 here and uninitialised memory there.
+        nz = self.z_size + 2
+        col = np.zeros(nz, dtype=self.dtype)
         val = 1
         for n_, i in enumerate(self.thickness):
             val_ = round(i / self.voxel_space)
-            vm[:, :, val:val_ + val] = np.int8(n_)
+            col[val:val_ + val] = np.int8(n_)
             val += val_
         self.end_point = np.int8(np.array(self.thickness).size)
-        for face in (np.s_[0, :, :], np.s_[-1, :, :], np.s_[:, 0, :], np.s_[:, -1, :],
-                     np.s_[:, :, 0], np.s_[:, :, -1]):
+        col[0] = self.end_point
+        col[-1] = self.end_point
+        vm = np.empty((self.x_size + 2, self.y_size + 2, nz), dtype=self.dtype)
+        vm[...] = col
+        for face in (np.s_[0, :, :], np.s_[-1, :, :], np.s_[:, 0, :], np.s_[:, -1, :]):
             vm[face] = self.end_point
         self.voxel_model = vm
 
@@ -570,7 +581,8 @@ class BaseVoxelMonteCarlo(metaclass=ABCMeta):
         dp = self._dprob
         fresh = torch.from_numpy(prob.labels).to(dp.device)
         if not torch.equal(fresh, dp.labels):
-            prob.validate()
+            prob.validate(labels=False)
+            E.check_labels(fresh, prob.end_label, prob.n_labels)
             dp.labels.copy_(fresh)
             if dp.words is not None:
                 dp.build_words()

@@ -181,3 +181,27 @@ def test_model_start_sees_in_place_volume_edit(cuda):
     assert np.array_equal(lab, vm.view(np.uint8))
     words = m._dprob.words.cpu().numpy().view(np.uint16)
     assert np.array_equal(words & 0xff, lab)
+
+
+def test_volume_checks_run_on_the_device_copy(cuda):
+    """The shell and label-range checks run on the uploaded labels: a broken
+    shell or a label without optics is refused with the host check's message,
+    both when a problem is uploaded and when start() finds an edited volume."""
+    from pymonteopt_b200 import VoxelPlateModel
+    good = _slab()
+    E.DeviceProblem(good)
+    for edit, msg in (((0, 5, 5), "shell"), ((5, 5, 5), "no optical properties")):
+        lab = good.labels.copy()
+        lab[edit] = 0 if msg == "shell" else 7
+        bad = pencil_problem(lab, 0.1, 1, [0.1], [10.0], [0.9], [1.37, 1.0])
+        with pytest.raises(ValueError, match=msg):
+            bad.validate()                       # host form of the same checks
+        with pytest.raises(ValueError, match=msg):
+            E.DeviceProblem(bad)
+    m = VoxelPlateModel(nPh=1000, keep_exits=False, verbose=False, device=cuda)
+    m.build(x_size=2.0, y_size=2.0, voxel_space=0.1, thickness=[1.0], n=[1.4], n_air=1.0,
+            ma=[0.1], ms=[10.0], g=[0.9])
+    m.start(1)
+    m.model.voxel_model[0, 3, 3] = 0
+    with pytest.raises(ValueError, match="shell"):
+        m.start(1)

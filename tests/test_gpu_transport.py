@@ -145,7 +145,7 @@ def _voxel_words_brute(labels, cap):
 def _build_words(lab, cap, cuda):
     d_lab = torch.from_numpy(lab).to(cuda)
     words = torch.empty(lab.shape, dtype=torch.int16, device=cuda)
-    scratch = torch.empty(3 * lab.size, dtype=torch.uint8, device=cuda)
+    scratch = torch.empty(A.PMO_VOXEL_WORDS_SCRATCH * lab.size, dtype=torch.uint8, device=cuda)
     st = load().pmo_build_voxel_words(d_lab.data_ptr(), *lab.shape, cap, words.data_ptr(),
                                       scratch.data_ptr(), scratch.numel(),
                                       torch.cuda.current_stream().cuda_stream)
@@ -191,6 +191,90 @@ def test_voxel_words_match_brute_force(cuda, cap, volume):
     if volume == "thin_layers":
         # the 1-voxel layer has d = 0 but a lateral reach of several voxels
         assert wd[10, 9, 3] == 0 and _lat(wc[10, 9, 3]) >= 6
+
+
+def _edge_sets(lab):
+    """E (a 26-neighbour of another label, or the array border) and E2 (an
+    in-plane 8-neighbour of another label, or the lateral border)."""
+    nx, ny, nz = lab.shape
+    p = np.pad(lab.astype(np.int32), 1, constant_values=-1)
+    E = np.zeros(lab.shape, bool)
+    E2 = np.zeros(lab.shape, bool)
+    for dx in (-1, 0, 1):
+        for dy in (-1, 0, 1):
+            for dz in (-1, 0, 1):
+                nb = p[1 + dx:1 + dx + nx, 1 + dy:1 + dy + ny, 1 + dz:1 + dz + nz]
+                diff = (nb != lab) & (nb >= 0)
+                E |= diff
+                if dz == 0:
+                    E2 |= diff
+    E2[0] = E2[-1] = True
+    E2[:, 0] = E2[:, -1] = True
+    E |= E2
+    E[:, :, 0] = E[:, :, -1] = True
+    return E, E2
+
+
+def _voxel_words_minmax(lab, cap):
+    """The words by separable min-max passes, vectorised (any size):
+    D(v) = min_{|k| <= K} max(|k|, D_prev(v + k e_axis)) per axis from 0 on
+    the edge set and 255 elsewhere; d = min(D, cap) over three axes, P over
+    x and y with K = 192; c from the smallest P over |dz| <= d."""
+    def dt(a, axis, K):
+        n = a.shape[axis]
+        out = a.copy()
+        for k in range(1, min(K, n - 1) + 1):
+            fwd = [slice(None)] * 3
+            bwd = [slice(None)] * 3
+            fwd[axis], bwd[axis] = slice(k, None), slice(0, n - k)
+            np.minimum(out[tuple(bwd)], np.maximum(a[tuple(fwd)], k), out=out[tuple(bwd)])
+            np.minimum(out[tuple(fwd)], np.maximum(a[tuple(bwd)], k), out=out[tuple(fwd)])
+        return out
+    E, E2 = _edge_sets(lab)
+    D = np.where(E, 0, 255).astype(np.int64)
+    for ax in range(3):
+        D = dt(D, ax, cap)
+    d = np.minimum(D, cap)
+    P = np.where(E2, 0, 255).astype(np.int64)
+    for ax in range(2):
+        P = dt(P, ax, 192)
+    nz = lab.shape[2]
+    e = np.full(lab.shape, 10**6, np.int64)
+    for k in range(-cap, cap + 1):
+        src = np.clip(np.arange(nz) + k, 0, nz - 1)
+        e = np.where(np.abs(k) <= d, np.minimum(e, P[:, :, src]), e)
+    c = np.zeros(lab.shape, np.int64)
+    for cc in range(1, 16):
+        c = np.where(_lat(cc) <= e, cc, c)
+    return lab.astype(np.int64) | d << 8 | c << 12
+
+
+@pytest.mark.parametrize("volume", ["wide_plate", "random_field"])
+def test_voxel_words_match_minmax_passes(cuda, volume):
+    """The builder counts edge voxels in boxes (summed-area tables and a
+    binary search); the restatement runs the min-max distance passes.  Equal
+    words on a plate wide enough for every lateral code (lat up to 192) and on
+    a random field."""
+    rng = np.random.default_rng(11)
+    if volume == "wide_plate":
+        lab = np.full((400, 390, 9), 3, np.uint8)
+        lab[1:-1, 1:-1, 1:3] = 0
+        lab[1:-1, 1:-1, 3:8] = 1
+        lab[200:203, 150:152, 4:6] = 2
+        lab[50, 300, 5] = 2
+    else:
+        f = rng.standard_normal((46, 41, 52))
+        for ax in range(3):
+            f = (f + np.roll(f, 1, ax) + np.roll(f, -1, ax)) / 3
+        lab = np.digitize(f, np.quantile(f, [0.3, 0.6, 0.8])).astype(np.uint8)
+        lab[0] = lab[-1] = 4
+        lab[:, 0] = lab[:, -1] = 4
+        lab[:, :, 0] = lab[:, :, -1] = 4
+    w = _build_words(lab, 15, cuda)
+    ref = _voxel_words_minmax(lab, 15)
+    assert np.array_equal(w, ref), int((w != ref).sum())
+    if volume == "wide_plate":
+        assert set(np.unique(w >> 12)) == set(range(16))
 
 
 @pytest.mark.parametrize("case", ["c1_small", "three_layer", "c3_small"])
