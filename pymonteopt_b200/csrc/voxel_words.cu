@@ -186,6 +186,9 @@ __global__ void depth_kernel(const uint32_t *__restrict__ sat, Grid3 g, uint32_t
             const uint32_t row = i / (uint32_t)g.nz;
             const int y = (int)(row % (uint32_t)g.ny), x = (int)(row / (uint32_t)g.ny);
             int lo = 1, hi = cap + 1;   // r = lo is uniform (v is not in E), r = hi is not tested
+            // most voxels of thick regions reach the cap: one count settles them
+            if (box_count(sat, g, x, y, z, cap - 1, cap - 1) == 0u) lo = cap;
+            else hi = cap;
             while (hi - lo > 1) {
                 const int mid = (lo + hi) >> 1;
                 if (box_count(sat, g, x, y, z, mid - 1, mid - 1) == 0u) lo = mid;
@@ -238,11 +241,10 @@ int pmo_build_voxel_words(const uint8_t *labels, int nx, int ny, int nz, int cap
     uint8_t *mask = reinterpret_cast<uint8_t *>(sat + total);
     const Grid3 g{nx, ny, nz};
     const uint32_t n = (uint32_t)total;
-    auto blocks_for = [](uint64_t threads) {
-        uint64_t b = (threads + 255) / 256;
-        if (b > 148ull * 32) b = 148ull * 32;
-        return (unsigned)(b ? b : 1);
-    };
+    // one thread (or warp) per item, no grid-stride reuse: blocks start in
+    // index order, so the probes of resident blocks sweep the table as one
+    // front along x and the planes they read stay in L2 between uses
+    auto blocks_for = [](uint64_t threads) { return (unsigned)((threads + 255) / 256); };
     const unsigned g_rows = blocks_for((uint64_t)nx * ny * 32);   // a warp per (x, y) row
     const unsigned g_vox = blocks_for(total);
     const uint32_t rows_y = (uint32_t)nx * nz, rows_x = (uint32_t)ny * nz;
