@@ -322,9 +322,25 @@ def main(argv=None) -> int:
     ap.add_argument("--reps", type=int, default=3)
     ap.add_argument("--warmup", type=int, default=1)
     ap.add_argument("--block-threads", type=int, default=0)
+    ap.add_argument("--words-reps", type=int, default=0,
+                    help="time this many uniform-box map builds instead of transport")
     args = ap.parse_args(argv)
     n = int(args.photons)
     dp = DeviceProblem(vols[args.volume]())
+    if args.words_reps > 0:
+        # the box map's build alone (the volume was uploaded and built once)
+        ts = []
+        for _ in range(args.words_reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            dp.build_words()
+            e1.record()
+            torch.cuda.synchronize()
+            ts.append(e0.elapsed_time(e1) / 1e3)
+        nvox = dp.labels.numel()
+        print(json.dumps({"volume": args.volume, "voxels": nvox, "words_seconds": min(ts),
+                          "voxels_per_s": nvox / min(ts)}))
+        return 0
     spec = TallySpec(nr=args.nr, dr=args.dr, fluence=flu[args.fluence])
     tallies = Tallies(dp, spec, n)
     best = float("inf")
