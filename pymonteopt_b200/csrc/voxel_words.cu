@@ -46,6 +46,8 @@
 //   4. d per voxel (binary search on the table of E), into the mask byte;
 //   5-7. the table again, for E2;
 //   8. c per voxel (binary search on the table of E2) and the word.
+// Passes 4 and 8 also run one warp per row, so that x and y are found once
+// per row rather than by divisions per voxel, and index in 32 bits.
 #include "pmo_internal.h"
 
 namespace {
@@ -158,67 +160,90 @@ struct Grid3 {
     int nx, ny, nz;
 };
 
-__device__ inline uint32_t sat_at(const uint32_t *__restrict__ s, const Grid3 &g, int x, int y,
-                                  int z) {
-    return (x < 0 || y < 0 || z < 0) ? 0u : __ldg(s + ((size_t)x * g.ny + y) * g.nz + z);
-}
-
-// edge voxels in [x-h, x+h] x [y-h, y+h] x [z-hz, z+hz], clipped to the array
+// Edge voxels in [x-h, x+h] x [y-h, y+h] x [z-hz, z+hz], clipped to the
+// array (h, hz >= 0).  The lower corners sit one below the box; a corner
+// below 0 reads as 0 and is skipped.  Every offset is below the voxel count,
+// hence below 2^32.
 __device__ inline uint32_t box_count(const uint32_t *__restrict__ s, const Grid3 &g, int x, int y,
                                      int z, int h, int hz) {
-    const int xa = max(x - h, 0) - 1, xb = min(x + h, g.nx - 1);
-    const int ya = max(y - h, 0) - 1, yb = min(y + h, g.ny - 1);
-    const int za = max(z - hz, 0) - 1, zb = min(z + hz, g.nz - 1);
-    return sat_at(s, g, xb, yb, zb) - sat_at(s, g, xa, yb, zb) - sat_at(s, g, xb, ya, zb) -
-           sat_at(s, g, xb, yb, za) + sat_at(s, g, xa, ya, zb) + sat_at(s, g, xa, yb, za) +
-           sat_at(s, g, xb, ya, za) - sat_at(s, g, xa, ya, za);
+    const int xa = x - h - 1, xb = min(x + h, g.nx - 1);
+    const int ya = y - h - 1, yb = min(y + h, g.ny - 1);
+    const int za = z - hz - 1, zb = min(z + hz, g.nz - 1);
+    const uint32_t ny = (uint32_t)g.ny, nz = (uint32_t)g.nz;
+    const uint32_t rbb = ((uint32_t)xb * ny + (uint32_t)yb) * nz;
+    uint32_t sum = __ldg(s + rbb + zb);
+    if (za >= 0) sum -= __ldg(s + rbb + za);
+    if (ya >= 0) {
+        const uint32_t rba = ((uint32_t)xb * ny + (uint32_t)ya) * nz;
+        sum -= __ldg(s + rba + zb);
+        if (za >= 0) sum += __ldg(s + rba + za);
+    }
+    if (xa >= 0) {
+        const uint32_t rab = ((uint32_t)xa * ny + (uint32_t)yb) * nz;
+        sum -= __ldg(s + rab + zb);
+        if (za >= 0) sum += __ldg(s + rab + za);
+        if (ya >= 0) {
+            const uint32_t raa = ((uint32_t)xa * ny + (uint32_t)ya) * nz;
+            sum += __ldg(s + raa + zb);
+            if (za >= 0) sum -= __ldg(s + raa + za);
+        }
+    }
+    return sum;
 }
 
-// Pass 4.  d into bits 2-5 of the mask.
-__global__ void depth_kernel(const uint32_t *__restrict__ sat, Grid3 g, uint32_t total, int cap,
+// Pass 4.  d into bits 2-5 of the mask.  One warp per (x, y) row, as in the
+// scans: x and y come once per row, a lane takes z = lane, lane + 32, ...
+__global__ void depth_kernel(const uint32_t *__restrict__ sat, Grid3 g, int cap,
                              uint8_t *__restrict__ mask) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total;
-         i += gridDim.x * blockDim.x) {
-        const uint8_t m = mask[i];
-        int d = 0;
-        if (!(m & 1) && cap > 0) {
-            const int z = (int)(i % (uint32_t)g.nz);
-            const uint32_t row = i / (uint32_t)g.nz;
-            const int y = (int)(row % (uint32_t)g.ny), x = (int)(row / (uint32_t)g.ny);
-            int lo = 1, hi = cap + 1;   // r = lo is uniform (v is not in E), r = hi is not tested
-            // most voxels of thick regions reach the cap: one count settles them
-            if (box_count(sat, g, x, y, z, cap - 1, cap - 1) == 0u) lo = cap;
-            else hi = cap;
-            while (hi - lo > 1) {
-                const int mid = (lo + hi) >> 1;
-                if (box_count(sat, g, x, y, z, mid - 1, mid - 1) == 0u) lo = mid;
-                else hi = mid;
+    const int lane = threadIdx.x & 31;
+    const uint32_t rows = (uint32_t)g.nx * (uint32_t)g.ny;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < rows; row += warps) {
+        const int x = (int)(row / (uint32_t)g.ny), y = (int)(row % (uint32_t)g.ny);
+        uint8_t *mrow = mask + (size_t)row * g.nz;
+        for (int z = lane; z < g.nz; z += 32) {
+            const uint8_t m = mrow[z];
+            int d = 0;
+            if (!(m & 1) && cap > 0) {
+                int lo = 1, hi = cap + 1;   // r = lo is uniform (v is not in E); r = hi is not
+                // most voxels of thick regions reach the cap: one count settles them
+                if (box_count(sat, g, x, y, z, cap - 1, cap - 1) == 0u) lo = cap;
+                else hi = cap;
+                while (hi - lo > 1) {
+                    const int mid = (lo + hi) >> 1;
+                    if (box_count(sat, g, x, y, z, mid - 1, mid - 1) == 0u) lo = mid;
+                    else hi = mid;
+                }
+                d = lo;
             }
-            d = lo;
+            mrow[z] = (uint8_t)((m & 3) | (d << 2));
         }
-        mask[i] = (uint8_t)((m & 3) | (d << 2));
     }
 }
 
-// Pass 8.  The lateral code and the word.
+// Pass 8.  The lateral code and the word; one warp per (x, y) row.
 __global__ void pack_kernel(const uint8_t *__restrict__ lab, const uint8_t *__restrict__ mask,
-                            const uint32_t *__restrict__ sat, Grid3 g, uint32_t total,
+                            const uint32_t *__restrict__ sat, Grid3 g,
                             uint16_t *__restrict__ words) {
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < total;
-         i += gridDim.x * blockDim.x) {
-        const int d = (mask[i] >> 2) & 15;
-        int lo = 0, hi = 16;   // code 0 needs no uniform square
-        if (!(mask[i] & 2)) {
-            const int z = (int)(i % (uint32_t)g.nz);
-            const uint32_t row = i / (uint32_t)g.nz;
-            const int y = (int)(row % (uint32_t)g.ny), x = (int)(row / (uint32_t)g.ny);
-            while (hi - lo > 1) {
-                const int mid = (lo + hi) >> 1;
-                if (box_count(sat, g, x, y, z, lat_of(mid) - 1, d) == 0u) lo = mid;
-                else hi = mid;
+    const int lane = threadIdx.x & 31;
+    const uint32_t rows = (uint32_t)g.nx * (uint32_t)g.ny;
+    const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+    for (uint32_t row = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; row < rows; row += warps) {
+        const int x = (int)(row / (uint32_t)g.ny), y = (int)(row % (uint32_t)g.ny);
+        const size_t base = (size_t)row * g.nz;
+        for (int z = lane; z < g.nz; z += 32) {
+            const uint8_t m = mask[base + z];
+            const int d = (m >> 2) & 15;
+            int lo = 0, hi = 16;   // code 0 needs no uniform square
+            if (!(m & 2)) {
+                while (hi - lo > 1) {
+                    const int mid = (lo + hi) >> 1;
+                    if (box_count(sat, g, x, y, z, lat_of(mid) - 1, d) == 0u) lo = mid;
+                    else hi = mid;
+                }
             }
+            words[base + z] = (uint16_t)(lab[base + z] | (d << 8) | (lo << 12));
         }
-        words[i] = (uint16_t)(lab[i] | (d << 8) | (lo << 12));
     }
 }
 
@@ -240,25 +265,24 @@ int pmo_build_voxel_words(const uint8_t *labels, int nx, int ny, int nz, int cap
     uint32_t *sat = static_cast<uint32_t *>(scratch);
     uint8_t *mask = reinterpret_cast<uint8_t *>(sat + total);
     const Grid3 g{nx, ny, nz};
-    const uint32_t n = (uint32_t)total;
-    // one thread (or warp) per item, no grid-stride reuse: blocks start in
-    // index order, so the probes of resident blocks sweep the table as one
-    // front along x and the planes they read stay in L2 between uses
+    // one warp per (x, y) row or one thread per strided row, no grid-stride
+    // reuse: blocks start in row order, so the probes of resident blocks
+    // sweep the table as one front along x and the planes they read stay in
+    // L2 between uses
     auto blocks_for = [](uint64_t threads) { return (unsigned)((threads + 255) / 256); };
     const unsigned g_rows = blocks_for((uint64_t)nx * ny * 32);   // a warp per (x, y) row
-    const unsigned g_vox = blocks_for(total);
     const uint32_t rows_y = (uint32_t)nx * nz, rows_x = (uint32_t)ny * nz;
     const size_t plane = (size_t)ny * nz;
     // d: table of E, then the binary search
     edge_scan_z_kernel<<<g_rows, 256, 0, s>>>(labels, nx, ny, nz, mask, sat);
     scan_strided_kernel<<<blocks_for(rows_y), 256, 0, s>>>(sat, rows_y, nz, plane, nz, ny);
     scan_strided_kernel<<<blocks_for(rows_x), 256, 0, s>>>(sat, rows_x, nz, nz, plane, nx);
-    depth_kernel<<<g_vox, 256, 0, s>>>(sat, g, n, cap, mask);
+    depth_kernel<<<g_rows, 256, 0, s>>>(sat, g, cap, mask);
     // c: table of E2, then the binary search and the words
     scan_z_bit_kernel<<<g_rows, 256, 0, s>>>(mask, nx, ny, nz, 1, sat);
     scan_strided_kernel<<<blocks_for(rows_y), 256, 0, s>>>(sat, rows_y, nz, plane, nz, ny);
     scan_strided_kernel<<<blocks_for(rows_x), 256, 0, s>>>(sat, rows_x, nz, nz, plane, nx);
-    pack_kernel<<<g_vox, 256, 0, s>>>(labels, mask, sat, g, n, words);
+    pack_kernel<<<g_rows, 256, 0, s>>>(labels, mask, sat, g, words);
     return cudaGetLastError() == cudaSuccess ? PMO_OK : PMO_ERR_CUDA;
 }
 
