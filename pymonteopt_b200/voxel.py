@@ -41,6 +41,18 @@ __all__ = ["VoxelPlateModel", "VoxelPlateExModel", "VoxelTuringModel", "VoxelArr
 # Volume models (host geometry builders)
 # =============================================================================
 
+def _host_volume(shape) -> np.ndarray:
+    """An uninitialised int8 host array for a label volume.  With a GPU
+    present it is page-locked memory from torch's caching host allocator:
+    a rebuilt model of the same size gets an already mapped block back (its
+    fill takes no page faults), and start() uploads it by direct DMA."""
+    import torch
+    if torch.cuda.is_available():
+        return torch.empty(tuple(int(s) for s in shape), dtype=torch.int8,
+                           pin_memory=True).numpy()
+    return np.empty(shape, dtype=np.int8)
+
+
 class VoxelModel:
     """Base of the geometry builders (pymopt/voxel_gpu/_classes.py:387-394)."""
 
@@ -119,8 +131,11 @@ class PlateModel(VoxelModel):
         self.end_point = np.int8(np.array(self.thickness).size)
         col[0] = self.end_point
         col[-1] = self.end_point
-        vm = np.empty((self.x_size + 2, self.y_size + 2, nz), dtype=self.dtype)
-        vm[...] = col
+        vm = _host_volume((self.x_size + 2, self.y_size + 2, nz))
+        # the broadcast copy runs on torch's CPU thread pool (numpy's is one
+        # thread); same bytes
+        import torch
+        torch.from_numpy(vm).copy_(torch.from_numpy(col).expand(vm.shape))
         for face in (np.s_[0, :, :], np.s_[-1, :, :], np.s_[:, 0, :], np.s_[:, -1, :]):
             vm[face] = self.end_point
         self.voxel_model = vm
