@@ -797,8 +797,13 @@ def main() -> int:
         model = VoxelPlateModel(nPh=photons, w_beam=V.C2_W_BEAM, keep_exits=False,
                                 verbose=False, nr=100, dr=0.1, device=dev,
                                 threadnum=args.block_threads or None)
-        model.build(**V.C2_PARAMS)
-        model.start(4999 + 7919 * rank)            # warm-up of the model path
+        # W untimed steps of the same path (the caching allocators, device and
+        # page-locked host, reach their steady state here)
+        for w_ in range(max(1, args.warmup)):
+            model.build(**V.C2_PARAMS)
+            model.start(4999 - w_ + 7919 * rank)
+            model.getRdTtValues()
+            model.get_Rr()
         e_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
                 for _ in range(args.steps)]
         e_wall = []
