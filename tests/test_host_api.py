@@ -29,6 +29,41 @@ def test_plate_volume_matches_reference():
     assert int(m.end_point) == 3
 
 
+def _plate_layer_by_layer(m):
+    """The reference's fill order (pymopt/voxel_gpu/_classes.py:437-457):
+    each layer's z slab, then the six shell faces."""
+    vm = np.zeros((m.x_size + 2, m.y_size + 2, m.z_size + 2), np.int8)
+    val = 1
+    for n_, t in enumerate(m.thickness):
+        k = round(t / m.voxel_space)
+        vm[:, :, val:val + k] = n_
+        val += k
+    e = len(m.thickness)
+    vm[0], vm[-1], vm[:, 0], vm[:, -1], vm[:, :, 0], vm[:, :, -1] = e, e, e, e, e, e
+    return vm
+
+
+def test_plate_volume_fill_matches_layer_by_layer():
+    """The column-broadcast fill gives the reference's bytes for random
+    stacks of one to five layers, and for the skin slab."""
+    from pymonteopt_b200 import volumes as V
+    rng = np.random.default_rng(3)
+    cases = [dict(V.C2_PARAMS)]
+    for k in rng.integers(1, 6, 12):
+        vs = float(rng.choice([0.05, 0.1, 0.2]))
+        cases.append(dict(x_size=float(rng.integers(3, 30)) * vs,
+                          y_size=float(rng.integers(3, 30)) * vs, voxel_space=vs,
+                          thickness=[float(t) * vs for t in rng.integers(1, 25, k)],
+                          n=[1.4] * k, n_air=1.0, ma=[0.1] * k, ms=[10.0] * k, g=[0.9] * k))
+    for c in cases:
+        m = VX.PlateModel()
+        m.verbose = False
+        m.set_params(**c)
+        m.build()
+        assert m.voxel_model.dtype == np.int8
+        assert np.array_equal(m.voxel_model, _plate_layer_by_layer(m)), c
+
+
 def test_plate_ex_volume_matches_reference():
     m = VX.PlateExModel()
     m.verbose = False
