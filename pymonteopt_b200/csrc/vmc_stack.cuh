@@ -27,6 +27,12 @@
 
 namespace pmo {
 
+// lanes at a plane that cross together (or fewer, when no lane can interact)
+#ifndef PMO_STACK_CROSS_BATCH
+#define PMO_STACK_CROSS_BATCH 8
+#endif
+constexpr int kStackCrossBatch = PMO_STACK_CROSS_BATCH;
+
 struct SParams {
     const pmo_stack *stacks;
     int32_t n_problems;
@@ -71,6 +77,13 @@ __global__ void __launch_bounds__(512) vmc_stack_kernel(const SParams sp) {
     int p = -1;
     uint32_t j = 0, k = 0, f = 0, ncr = 0;
     R x = 0, y = 0, z = 0, vx = 0, vy = 0, vz = 1, w = 0, wseg = 0;
+    // the flight in progress: drawn from Philox block k - 1, st optical depth
+    // left, ry the block's spare word (free until a Fresnel decision or the
+    // roulette takes it).  A flight may span several passes of the feed
+    // loop, one plane crossing per pass.
+    R st = 0;
+    uint32_t ry = 0;
+    bool flying = false, ry_free = false;
     // layer state: current layer li of nl (rows l0 + i of the table), its
     // planes z_top < z_bot, its index and optics; Lc, Nc: path length and
     // interactions in the current layer since the photon entered it
@@ -99,6 +112,7 @@ __global__ void __launch_bounds__(512) vmc_stack_kernel(const SParams sp) {
         p = pp;
         j = jj;
         k = f = ncr = 0;
+        flying = false;
         const pmo_stack st = sp.stacks[pp];
         l0 = st.first_layer;
         nl = (int)st.n_layers;
@@ -134,145 +148,148 @@ __global__ void __launch_bounds__(512) vmc_stack_kernel(const SParams sp) {
         return true;
     };
 
-    // one interaction cycle; returns true while the photon is in flight
-    auto cycle = [&]() -> bool {
-        const uint4 rn = philox4x32_10(make_uint4(k, 4u * (uint32_t)p, j, 0u), sp.rk);
-        ++k;
-        R st = pneglog(u01<R>(rn.x));
-        // rn.y is the step's spare uniform: the first Fresnel decision with
-        // 0 < ra < 1 or the roulette takes it, as in the plain kernel
-        bool ry_free = true;
-        for (;;) {
-            // distance to the plane ahead in the photon's layer
-            const R dzf = vz > R(0) ? xsub(z_bot, z) : (vz < R(0) ? xsub(z_top, z) : R(0));
-            const R db = vz != R(0) ? xdiv(dzf, vz) : R(1e30);
-            const R dbmt = xmul(db, hg.mt);
-            if (!(st >= dbmt)) {
-                const R s = xmul(st, hg.imt);
-                x = xfma(vx, s, x);
-                y = xfma(vy, s, y);
-                z = xfma(vz, s, z);
-                Lc = xadd(Lc, s);
-                break;
-            }
-            x = xfma(vx, db, x);
-            y = xfma(vy, db, y);
-            z = vz > R(0) ? z_bot : z_top;
-            Lc = xadd(Lc, db);
-            st = xsub(st, dbmt);
-            ++ncr;
-            if (ncr + k - 1 > cap) {
-                gadd(p, PMO_SS_ERRW, (double)w);
-                finish();
-                return false;
-            }
-            // the layer (or the ambient medium) across the plane
-            const int nxt = vz > R(0) ? li + 1 : li - 1;
-            const bool out = nxt < 0 || nxt >= nl;
-            const R nn = out ? n_amb : (R)sp.layers[l0 + nxt].n;
-            bool transmit = true;
-            R cb = R(1), nr = R(1);
-            if (ncur != nn) {
-                // Fresnel / total internal reflection (:105-153)
-                const uint32_t fk = f++;   // this decision's Philox counter
-                R ca = fabs(vz);
-                if (ca > R(1)) ca = R(1);
-                nr = xdiv(ncur, nn);
-                const R sa = psqrt(xfma(-ca, ca, R(1)));
-                const R sb = xmul(nr, sa);
-                R ra;
-                if (ncur > nn && sb >= R(1)) {
-                    ra = R(1);
+    // the plane ahead in the photon's layer: distance db, optical depth dbmt
+    auto plane_ahead = [&](R &db, R &dbmt) {
+        const R dzf = vz > R(0) ? xsub(z_bot, z) : (vz < R(0) ? xsub(z_top, z) : R(0));
+        db = vz != R(0) ? xdiv(dzf, vz) : R(1e30);
+        dbmt = xmul(db, hg.mt);
+    };
+
+    // one plane crossing of the flight (st >= dbmt): the photon moves to the
+    // plane, then reflects, enters the next layer or leaves; the flight goes
+    // on with the optical depth left.  Returns true while the photon is in
+    // flight.
+    auto cross = [&](R db, R dbmt) -> bool {
+        x = xfma(vx, db, x);
+        y = xfma(vy, db, y);
+        z = vz > R(0) ? z_bot : z_top;
+        Lc = xadd(Lc, db);
+        st = xsub(st, dbmt);
+        ++ncr;
+        if (ncr + k - 1 > cap) {
+            gadd(p, PMO_SS_ERRW, (double)w);
+            finish();
+            return false;
+        }
+        // the layer (or the ambient medium) across the plane
+        const int nxt = vz > R(0) ? li + 1 : li - 1;
+        const bool out = nxt < 0 || nxt >= nl;
+        const R nn = out ? n_amb : (R)sp.layers[l0 + nxt].n;
+        bool transmit = true;
+        R cb = R(1), nr = R(1);
+        if (ncur != nn) {
+            // Fresnel / total internal reflection (:105-153)
+            const uint32_t fk = f++;   // this decision's Philox counter
+            R ca = fabs(vz);
+            if (ca > R(1)) ca = R(1);
+            nr = xdiv(ncur, nn);
+            const R sa = psqrt(xfma(-ca, ca, R(1)));
+            const R sb = xmul(nr, sa);
+            R ra;
+            if (ncur > nn && sb >= R(1)) {
+                ra = R(1);
+            } else {
+                cb = psqrt(xfma(-sb, sb, R(1)));
+                if (ca == R(1)) {
+                    ra = R(0);
                 } else {
-                    cb = psqrt(xfma(-sb, sb, R(1)));
-                    if (ca == R(1)) {
-                        ra = R(0);
-                    } else {
-                        const R cacb = xmul(ca, cb), sasb = xmul(sa, sb);
-                        const R sacb = xmul(sa, cb), casb = xmul(ca, sb);
-                        const R cap_ = xsub(cacb, sasb), cam = xadd(cacb, sasb);
-                        const R sap = xadd(sacb, casb), sam = xsub(sacb, casb);
-                        const R num = xmul(xmul(xmul(R(0.5), sam), sam),
-                                           xfma(cap_, cap_, xmul(cam, cam)));
-                        const R den = xmul(xmul(xmul(sap, sap), cam), cam);
-                        ra = xdiv(num, den);
-                    }
-                }
-                // transmit when ra < u (:150); only 0 < ra < 1 needs u, which
-                // is the step's spare word while free, else draw (fk, 1)
-                if (ra > R(0) && ra < R(1)) {
-                    uint32_t word = rn.y;
-                    if (!ry_free)
-                        word = philox4x32_10(make_uint4(fk, 1u + 4u * (uint32_t)p, j, 0u),
-                                             sp.rk).x;
-                    ry_free = false;
-                    transmit = ra < u01<R>(word);
-                } else {
-                    transmit = ra <= R(0);
+                    const R cacb = xmul(ca, cb), sasb = xmul(sa, sb);
+                    const R sacb = xmul(sa, cb), casb = xmul(ca, sb);
+                    const R cap_ = xsub(cacb, sasb), cam = xadd(cacb, sasb);
+                    const R sap = xadd(sacb, casb), sam = xsub(sacb, casb);
+                    const R num = xmul(xmul(xmul(R(0.5), sam), sam),
+                                       xfma(cap_, cap_, xmul(cam, cam)));
+                    const R den = xmul(xmul(xmul(sap, sap), cam), cam);
+                    ra = xdiv(num, den);
                 }
             }
-            if (!transmit) {
-                vz = -vz;   // reflect and stay in the layer (:150-152)
-                continue;
+            // transmit when ra < u (:150); only 0 < ra < 1 needs u, which
+            // is the step's spare word while free, else draw (fk, 1)
+            if (ra > R(0) && ra < R(1)) {
+                uint32_t word = ry;
+                if (!ry_free)
+                    word = philox4x32_10(make_uint4(fk, 1u + 4u * (uint32_t)p, j, 0u),
+                                         sp.rk).x;
+                ry_free = false;
+                transmit = ra < u01<R>(word);
+            } else {
+                transmit = ra <= R(0);
             }
-            if (ncur != nn) {
-                // refracted direction (:124-134)
-                vx = xmul(vx, nr);
-                vy = xmul(vy, nr);
-                vz = xmul(sgn(vz), cb);
-                const R inv = pinvnorm(sumsq(vx, vy, vz));
-                vx = xmul(vx, inv);
-                vy = xmul(vy, inv);
-                vz = xmul(vz, inv);
+        }
+        if (!transmit) {
+            vz = -vz;   // reflect and stay in the layer (:150-152)
+            return true;
+        }
+        if (ncur != nn) {
+            // refracted direction (:124-134)
+            vx = xmul(vx, nr);
+            vy = xmul(vy, nr);
+            vz = xmul(sgn(vz), cb);
+            const R inv = pinvnorm(sumsq(vx, vy, vz));
+            vx = xmul(vx, inv);
+            vy = xmul(vy, inv);
+            vz = xmul(vz, inv);
+        }
+        flush_layer();
+        if (out) {
+            // exit: Rd or Tt with the per-layer derivative sums, R(r)
+            const double wd = (double)w;
+            const bool top = vz < R(0);
+            gadd(p, top ? PMO_SS_RD : PMO_SS_TT, wd);
+            const int off = top ? 0 : 2;
+            for (int i = 0; i < nl; ++i) {
+                gadd(p, PMO_SS_LAYER0 + 4 * i + off, wd * (double)accL[i]);
+                gadd(p, PMO_SS_LAYER0 + 4 * i + off + 1, wd * (double)accN[i]);
             }
-            flush_layer();
-            if (out) {
-                // exit: Rd or Tt with the per-layer derivative sums, R(r)
-                const double wd = (double)w;
-                const bool top = vz < R(0);
-                gadd(p, top ? PMO_SS_RD : PMO_SS_TT, wd);
-                const int off = top ? 0 : 2;
-                for (int i = 0; i < nl; ++i) {
-                    gadd(p, PMO_SS_LAYER0 + 4 * i + off, wd * (double)accL[i]);
-                    gadd(p, PMO_SS_LAYER0 + 4 * i + off + 1, wd * (double)accN[i]);
-                }
-                if (top && sp.nr > 0) {
-                    const R r = psqrt(xfma(y, y, xmul(x, x)));
-                    if (r > R(0)) {
-                        const R q = ceil(xdiv(r, dr));
-                        if (q >= R(1) && q <= (R)sp.nr) {
-                            float *b = sp.bins + ((size_t)p * sp.nr + ((int)q - 1)) * PMO_SB_N;
-                            atomicAdd(b, (float)wd);
-                            for (int i = 0; i < nl; ++i) {
-                                const double a = wd * (double)accL[i];
-                                const double c = wd * (double)accN[i];
-                                if (a != 0.0) atomicAdd(b + 1 + 2 * i, (float)a);
-                                if (c != 0.0) atomicAdd(b + 2 + 2 * i, (float)c);
-                            }
+            if (top && sp.nr > 0) {
+                const R r = psqrt(xfma(y, y, xmul(x, x)));
+                if (r > R(0)) {
+                    const R q = ceil(xdiv(r, dr));
+                    if (q >= R(1) && q <= (R)sp.nr) {
+                        float *b = sp.bins + ((size_t)p * sp.nr + ((int)q - 1)) * PMO_SB_N;
+                        atomicAdd(b, (float)wd);
+                        for (int i = 0; i < nl; ++i) {
+                            const double a = wd * (double)accL[i];
+                            const double c = wd * (double)accN[i];
+                            if (a != 0.0) atomicAdd(b + 1 + 2 * i, (float)a);
+                            if (c != 0.0) atomicAdd(b + 2 + 2 * i, (float)c);
                         }
                     }
                 }
-                finish();
-                return false;
             }
-            // enter the next layer; the remaining optical depth carries over
-            li = nxt;
-            set_layer(li);
-            const R t = (R)sp.layers[l0 + li].thickness;
-            if (vz > R(0)) {
-                z_top = z_bot;
-                z_bot = xadd(z_top, t);
-            } else {
-                z_bot = z_top;
-                z_top = xsub(z_bot, t);
-            }
+            finish();
+            return false;
         }
+        // enter the next layer; the remaining optical depth carries over
+        li = nxt;
+        set_layer(li);
+        const R t = (R)sp.layers[l0 + li].thickness;
+        if (vz > R(0)) {
+            z_top = z_bot;
+            z_bot = xadd(z_top, t);
+        } else {
+            z_bot = z_top;
+            z_top = xsub(z_bot, t);
+        }
+        return true;
+    };
+
+    // the end of the flight inside the layer: hop, absorption, roulette and
+    // spin, the last two from the words rz, rw of the flight's block.
+    // Returns true while the photon is in flight.
+    auto interact = [&](uint32_t rz, uint32_t rw) -> bool {
+        const R s = xmul(st, hg.imt);
+        x = xfma(vx, s, x);
+        y = xfma(vy, s, y);
+        z = xfma(vz, s, z);
+        Lc = xadd(Lc, s);
+        flying = false;
         Nc = xadd(Nc, R(1));
         // absorption (:179)
         w = xfma(-w, hg.ma_mt, w);
         // roulette (:182-195): the spare word, or draw (k - 1, 3)
         if (w <= R(0.0001)) {
-            uint32_t word = rn.y;
+            uint32_t word = ry;
             if (!ry_free)
                 word = philox4x32_10(make_uint4(k - 1u, 3u + 4u * (uint32_t)p, j, 0u), sp.rk).x;
             if (R(0.1) < u01<R>(word)) {
@@ -287,11 +304,11 @@ __global__ void __launch_bounds__(512) vmc_stack_kernel(const SParams sp) {
         }
         // spin (:197-219)
         {
-            const R ct = hg_cos<R>(hg, u01<R>(rn.z));
+            const R ct = hg_cos<R>(hg, u01<R>(rz));
             const R s2 = xfma(-ct, ct, R(1));
             const R sth = psqrt(s2 > R(0) ? s2 : R(0));
             R sf, cf;
-            psincos2pi(u01<R>(rn.w), &sf, &cf);
+            psincos2pi(u01<R>(rw), &sf, &cf);
             if (R(0.99999) < fabs(vz)) {
                 const R sz = sgn(vz);
                 vx = xmul(sth, cf);
@@ -351,7 +368,41 @@ __global__ void __launch_bounds__(512) vmc_stack_kernel(const SParams sp) {
             need &= ~taken;
         }
         if (!__any_sync(FULL, active || more)) break;
-        if (active) active = cycle();
+        // One pass: a lane without a flight draws one (block k, as the slab
+        // kernel); then it either ends the flight inside its layer or, at a
+        // plane, crosses it.  Lanes at a plane cross together once
+        // kStackCrossBatch of them wait, or when no lane can interact; else
+        // they wait a pass.  Every lane meets the next pass's ballots, so the
+        // warp runs the interaction code whole after any crossing.
+        R db = R(0), dbmt = R(0);
+        uint4 rn = make_uint4(0u, 0u, 0u, 0u);
+        bool fresh = false, at_plane = false;
+        if (active) {
+            if (!flying) {
+                rn = philox4x32_10(make_uint4(k, 4u * (uint32_t)p, j, 0u), sp.rk);
+                ++k;
+                st = pneglog(u01<R>(rn.x));
+                ry = rn.y;
+                ry_free = true;
+                flying = fresh = true;
+            }
+            plane_ahead(db, dbmt);
+            at_plane = st >= dbmt;
+        }
+        const unsigned waiting = __ballot_sync(FULL, at_plane);
+        const bool go = __popc(waiting) >= kStackCrossBatch ||
+                        __ballot_sync(FULL, active && !at_plane) == 0u;
+        if (active) {
+            if (!at_plane) {
+                // the block's last two words: in registers when it was drawn
+                // this pass, else drawn again (after a crossing or a wait)
+                if (!fresh)
+                    rn = philox4x32_10(make_uint4(k - 1u, 4u * (uint32_t)p, j, 0u), sp.rk);
+                active = interact(rn.z, rn.w);
+            } else if (go) {
+                active = cross(db, dbmt);
+            }
+        }
     }
 }
 
