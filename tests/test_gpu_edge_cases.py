@@ -205,3 +205,27 @@ def test_volume_checks_run_on_the_device_copy(cuda):
     m.model.voxel_model[0, 3, 3] = 0
     with pytest.raises(ValueError, match="shell"):
         m.start(1)
+
+
+def test_plate_volume_is_page_locked_and_exact(cuda):
+    """With a GPU present a plate volume is built in page-locked memory (the
+    upload is then a direct copy); its bytes are still the reference's
+    layer-by-layer fill, on a first build and on a rebuild of the same size
+    (a reused block)."""
+    from pymonteopt_b200 import voxel as VX
+    params = dict(x_size=3.1, y_size=2.7, voxel_space=0.1, thickness=[0.2, 0.9, 0.4],
+                  n=[1.4, 1.37, 1.45], n_air=1.0, ma=[0.1, 0.2, 0.3], ms=[10, 20, 30],
+                  g=[0.9, 0.8, 0.7])
+    m = VX.PlateModel()
+    m.verbose = False
+    m.set_params(**params)
+    for _ in range(2):
+        m.build()
+        vm = m.voxel_model
+        assert torch.from_numpy(vm).is_pinned()
+        ref = np.zeros(vm.shape, np.int8)
+        ref[:, :, 1:3], ref[:, :, 3:12], ref[:, :, 12:16] = 0, 1, 2
+        ref[0] = ref[-1] = 3
+        ref[:, 0] = ref[:, -1] = 3
+        ref[:, :, 0] = ref[:, :, -1] = 3
+        assert vm.shape == (33, 29, 17) and np.array_equal(vm, ref)
