@@ -45,7 +45,8 @@ def _host_volume(shape) -> np.ndarray:
     """An uninitialised int8 host array for a label volume.  With a GPU
     present it is page-locked memory from torch's caching host allocator:
     a rebuilt model of the same size gets an already mapped block back (its
-    fill takes no page faults), and start() uploads it by direct DMA."""
+    fill takes no page faults), and start() uploads it by direct DMA.  The
+    allocation initialises CUDA in the process, which start() does anyway."""
     import torch
     if torch.cuda.is_available():
         return torch.empty(tuple(int(s) for s in shape), dtype=torch.int8,
