@@ -256,9 +256,10 @@ class SlabBatch:
         else:
             by_mode = {modes[0]: shapes[shape]}
         # contention only grows with the budgets, so the down-scaled timing
-        # flatters global atomics: they must win clearly to be kept
+        # flatters global atomics (on C5: 1-3 % ahead at 1/8, 25 % behind at
+        # full size): they must win by 10 % to be kept
         mode = modes[0]
-        if len(modes) > 1 and by_mode[A.PMO_BT_GLOBAL] < 0.97 * by_mode[A.PMO_BT_THREAD]:
+        if len(modes) > 1 and by_mode[A.PMO_BT_GLOBAL] < 0.90 * by_mode[A.PMO_BT_THREAD]:
             mode = A.PMO_BT_GLOBAL
         best = (*shape, mode)
         self.tune_table = {"best": best, "shape_ms": {str(k): v for k, v in shapes.items()},
