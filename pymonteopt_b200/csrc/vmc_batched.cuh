@@ -95,6 +95,7 @@ __global__ void __launch_bounds__(512) vmc_batched_kernel(const BParams bp) {
     int p = -1;
     uint32_t j = 0, k = 0, f = 0, ncr = 0;
     R x = 0, y = 0, z = 0, vx = 0, vy = 0, vz = 1, w = 0, wseg = 0, L = 0;
+    PhiloxFixed pfix{0u, 0u, 0u};   // the photon's fixed part of its interaction draws
     // add v to sum `slot` of the photon's problem
     auto add = [&](int slot, double v) {
         if (priv) acc[slot] += v;
@@ -112,6 +113,7 @@ __global__ void __launch_bounds__(512) vmc_batched_kernel(const BParams bp) {
         p = pp;
         j = jj;
         k = f = ncr = 0;
+        pfix = philox_fixed(4u * (uint32_t)pp, jj, bp.rk);
         const pmo_slab sl = bp.slabs[pp];
         make_props<R>(hg, sl.ma, sl.ms, sl.g, sl.n_tissue);
         mt = hg.mt;
@@ -148,7 +150,7 @@ __global__ void __launch_bounds__(512) vmc_batched_kernel(const BParams bp) {
 
     // one interaction cycle; returns true while the photon is in flight
     auto cycle = [&]() -> bool {
-        const uint4 rn = philox4x32_10(make_uint4(k, 4u * (uint32_t)p, j, 0u), bp.rk);
+        const uint4 rn = philox4x32_10_fixed(k, 0u, pfix, bp.rk);
         ++k;
         R st = pneglog(u01<R>(rn.x));
         // rn.y is the step's spare uniform: the first Fresnel decision with

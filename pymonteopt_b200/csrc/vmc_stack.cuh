@@ -77,6 +77,7 @@ __global__ void __launch_bounds__(512) vmc_stack_kernel(const SParams sp) {
     int p = -1;
     uint32_t j = 0, k = 0, f = 0, ncr = 0;
     R x = 0, y = 0, z = 0, vx = 0, vy = 0, vz = 1, w = 0, wseg = 0;
+    PhiloxFixed pfix{0u, 0u, 0u};   // the photon's fixed part of its interaction draws
     // the flight in progress: drawn from Philox block k - 1, st optical depth
     // left, ry the block's spare word (free until a Fresnel decision or the
     // roulette takes it).  A flight may span several passes of the feed
@@ -112,6 +113,7 @@ __global__ void __launch_bounds__(512) vmc_stack_kernel(const SParams sp) {
         p = pp;
         j = jj;
         k = f = ncr = 0;
+        pfix = philox_fixed(4u * (uint32_t)pp, jj, sp.rk);
         flying = false;
         const pmo_stack st = sp.stacks[pp];
         l0 = st.first_layer;
@@ -379,7 +381,7 @@ __global__ void __launch_bounds__(512) vmc_stack_kernel(const SParams sp) {
         bool fresh = false, at_plane = false;
         if (active) {
             if (!flying) {
-                rn = philox4x32_10(make_uint4(k, 4u * (uint32_t)p, j, 0u), sp.rk);
+                rn = philox4x32_10_fixed(k, 0u, pfix, sp.rk);
                 ++k;
                 st = pneglog(u01<R>(rn.x));
                 ry = rn.y;
@@ -397,7 +399,7 @@ __global__ void __launch_bounds__(512) vmc_stack_kernel(const SParams sp) {
                 // the block's last two words: in registers when it was drawn
                 // this pass, else drawn again (after a crossing or a wait)
                 if (!fresh)
-                    rn = philox4x32_10(make_uint4(k - 1u, 4u * (uint32_t)p, j, 0u), sp.rk);
+                    rn = philox4x32_10_fixed(k - 1u, 0u, pfix, sp.rk);
                 active = interact(rn.z, rn.w);
             } else if (go) {
                 active = cross(db, dbmt);
